@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""Benchmark of the unified-particle step on B200 (one JSON line on stdout).
+
+Workload (one "step" = one frame of 5 substeps x 3 Jacobi iterations):
+the reference's GPU default scene — a 20^3 = 8,000-particle body with
+93,556 distance constraints and 65,536 fluid particles (deriveOpts(20,
+65536, 30), seeded jittered block), with one slice wedge through the body
+centre at frame 60 of the timed run.
+
+  value        particle-substeps/s with the state resident in HBM, device
+               time (CUDA events per frame, L2 flushed between frames),
+               summed over all ranks (each rank steps its own replica)
+  e2e          the same metric through the C ABI the way a Solver user
+               drives it: per frame the uniform block goes host->device and
+               positions + flags come back device->host into pinned memory
+  roofline     the dominant kernel's algorithmic bytes per launch over its
+               average event-timed duration, against the measured HBM peak
+  cpu_baseline the CPU solver restated (oracle O1, src/solver.js numerics),
+               single thread as JavaScript runs, on a bounded sample
+  clocks       nvidia-smi samples taken during the timed region
+
+`--impl reference` times the reference's CPU implementation of the step
+(O1, one substep per step) on this host instead and prints its line.
+Launch for N GPUs: python -m torch.distributed.run --nproc-per-node N bench.py --gpus N
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-substeps/s plain vs batched; HBM GB/s %peak; p50/p99 served frame ms"
+UNIT = "particle-substeps/s"
+
+# Algorithmic bytes per processed element of each kernel: every array a pass
+# reads or writes counted once, neighbour re-reads counted as cache hits.
+# Units: A = active particles, F = active fluid, S = solids, C = constraints,
+# T = hash buckets.
+KERNEL_BYTES = {
+    "integrate_count": lambda u: 96 * u["A"],
+    "scan": lambda u: 8 * u["T"],
+    "scatter": lambda u: 20 * u["A"],
+    "rankfix": lambda u: 16 * u["A"],
+    "density": lambda u: 28 * u["F"],
+    "disp": lambda u: 40 * u["F"],
+    "apply_fluid": lambda u: 48 * u["F"],
+    "solid_solve": lambda u: 36 * u["S"] + 24 * u["C"],
+    "apply_solid": lambda u: 48 * u["S"],
+    "bond_contacts": lambda u: 20 * u["C"] + 40 * u["A"],
+    "apply_bounds_vel": lambda u: 84 * u["A"],
+    "xsph": lambda u: 52 * u["F"],
+    "xsph_apply": lambda u: 32 * u["F"],
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from a committed ncu summary, if one exists:
+    profiles/traffic.txt lines `kernel workload bytes_per_launch`."""
+    f = ROOT / "profiles" / "traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(seconds: float = 12.0) -> dict:
+    """O1 (the CPU solver restated with its JavaScript numerics) on the
+    default scene, one thread, a bounded number of substeps from the
+    scene's initial state."""
+    from fluidphysics_b200 import scenes as S
+    from oracle.oracle import o1_from_scene
+    sc = S.gpu_default(frames=1)
+    o1 = o1_from_scene(sc)
+    h = sc.dt / sc.substeps
+    n_sub = 0
+    parts = 0
+    t0 = time.perf_counter()
+    while True:
+        act = int(o1.get("active").sum())
+        o1.step(h, 1)
+        n_sub += 1
+        parts += act
+        el = time.perf_counter() - t0
+        if el >= seconds or n_sub >= 500:
+            break
+    return {"value": parts / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n_sub} substeps of gpu_default (8,000 body + 65,536 fluid) from its initial "
+                      f"state, O1 restatement of src/solver.js, 1 thread, {el:.1f} s"}
+
+
+def run_reference(args) -> None:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from fluidphysics_b200 import scenes as S
+    from oracle.oracle import o1_from_scene
+    sc = S.gpu_default(frames=1)
+    o1 = o1_from_scene(sc)
+    h = sc.dt / sc.substeps
+    for _ in range(args.warmup):
+        o1.step(h, 1)
+    parts = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        parts += int(o1.get("active").sum())
+        o1.step(h, 1)
+    el = time.perf_counter() - t0
+    v = parts / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded jittered fluid block, lattice body)",
+        "config": {"workload": "gpu_default: 20^3 body (93,556 constraints) + 65,536 fluid, 1 substep "
+                               "per step (h = 1/300), CPU solver", "substeps_per_step": 1},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"{args.steps} substeps of gpu_default with O1, the restatement of "
+                                   "src/solver.js (no JavaScript engine on this host), 1 thread"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="upbd", choices=["upbd", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--profile-frames", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    from fluidphysics_b200 import _lib as L
+    from fluidphysics_b200 import scenes as S
+    from fluidphysics_b200.sim import sim_from_scene
+
+    sc = S.gpu_default(frames=args.steps)
+    sc.desc.device = local
+    sim = sim_from_scene(sc)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    init = sim.read_state()
+    init_cons = sim.read_constraints()
+    info = sim.info
+    T = info.table_size
+
+    # L2 flush buffer: twice the 126 MB L2
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def do_flush():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+
+    def reset():
+        sim.write_state(**init)
+        sim.write_constraints(init_cons)
+
+    # warm-up (graphs captured here), then back to the initial state
+    for _ in range(args.warmup):
+        sim.step(sc.dt, sc.substeps)
+    sim.sync()
+    reset()
+
+    # ---- timed region: K frames, device time per frame, L2 flushed between
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    cvd = [x for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+    phys = int(cvd[local]) if local < len(cvd) and cvd[local].strip().isdigit() else local
+    clocks = Clocks(phys)
+    launches0 = sim.launches
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(K):
+        do_flush()
+        ev[k][0].record(stream)
+        if k == sc.slice_frame:
+            sim.slice(*sc.wedge)
+        sim.step(sc.dt, sc.substeps)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    launches = sim.launches - launches0
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    sim.sync()
+    active = info.solid_n + sim.active_count()
+    local_units = active * sc.substeps * K
+    t_max = ms
+    units = local_units
+    if pg:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max = float(t.item())
+        u = torch.tensor([local_units], device="cuda", dtype=torch.float64)
+        pg.all_reduce(u, op=pg.ReduceOp.SUM)
+        units = float(u.item())
+    value = units / (t_max / 1e3)
+
+    # ---- e2e through the C ABI with pinned host buffers
+    reset()
+    E = min(args.e2e_steps, K)
+    pos_h = torch.empty((info.total, 4), dtype=torch.float32, pin_memory=True)
+    flags_h = torch.empty(info.total, dtype=torch.int32, pin_memory=True)
+    import ctypes as C
+    fp = C.cast(pos_h.data_ptr(), C.POINTER(C.c_float))
+    up = C.cast(flags_h.data_ptr(), C.POINTER(C.c_uint32))
+    for _ in range(3):  # warm the readback path
+        sim.step(sc.dt, sc.substeps)
+        L.check(sim.lib, sim.h, sim.lib.upbd_read_state(sim.h, fp, None, None, None, up))
+    reset()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(E):
+        if k == sc.slice_frame:
+            sim.slice(*sc.wedge)
+        sim.step(sc.dt, sc.substeps)
+        L.check(sim.lib, sim.h, sim.lib.upbd_read_state(sim.h, fp, None, None, None, up))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_units = active * sc.substeps * E * ws
+    e2e_value = e2e_units / (e2e_ms / 1e3)
+
+    # ---- per-kernel device times of eager frames (dominant kernel roofline)
+    reset()
+    for _ in range(30):  # into a settled, interacting state
+        sim.step(sc.dt, sc.substeps)
+    sim.sync()
+    P = args.profile_frames
+    tot = np.zeros(L.KERNEL_KINDS)
+    cnt = np.zeros(L.KERNEL_KINDS)
+    msb = (C.c_double * L.KERNEL_KINDS)()
+    lnb = (C.c_uint32 * L.KERNEL_KINDS)()
+    for _ in range(P):
+        do_flush()
+        torch.cuda.synchronize()
+        L.check(sim.lib, sim.h, sim.lib.upbd_profile_frame(sim.h, sc.dt, sc.substeps, msb, lnb))
+        tot += np.array(msb[:])
+        cnt += np.array(lnb[:])
+    names = [(sim.lib.upbd_kernel_name(k) or b"").decode() for k in range(L.KERNEL_KINDS)]
+    st = sim.read_state()
+    n_act = int((st["flags"] & 1).sum())
+    n_fl = int((st["flags"][info.solid_n:] & 1).sum())
+    units_k = {"A": n_act, "F": n_fl, "S": info.solid_n, "C": info.num_cons, "T": T}
+    per_kernel = {}
+    for k, nm in enumerate(names):
+        if cnt[k] > 0 and nm:
+            avg_ms = tot[k] / cnt[k]
+            b = KERNEL_BYTES[nm](units_k) if nm in KERNEL_BYTES else None
+            per_kernel[nm] = {"share": tot[k] / tot.sum(), "avg_us": avg_ms * 1e3,
+                              "launches_per_frame": cnt[k] / P,
+                              "gbs": (b / (avg_ms / 1e3) / 1e9) if b else None}
+    dom = max((nm for nm in per_kernel if nm in KERNEL_BYTES), key=lambda n: per_kernel[n]["share"])
+    peaks, peak_src = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    dk = per_kernel[dom]
+    achieved = dk["gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_src == "measured" else "fallback 6.65 TB/s",
+                "bytes_per_launch": KERNEL_BYTES[dom](units_k), "avg_launch_us": dk["avg_us"],
+                "traffic": ncu_traffic(dom, "gpu_default"),
+                "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                            for k, v in sorted(per_kernel.items(), key=lambda x: -x[1]["share"])}}
+    # whole-step roofline: the substep's algorithmic bytes at the measured rate
+    B_sub = (240 * n_act + 200 * n_fl + 8 * T + sc.desc.solid_iters * (84 * info.solid_n + 24 * info.num_cons)
+             + 20 * info.num_cons)
+    step_gbs = B_sub * sc.substeps * K / (ms / 1e3) / 1e9
+    roofline["step_achieved_gbs"] = step_gbs
+    roofline["step_frac"] = step_gbs / hbm
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(args.cpu_seconds)
+        except Exception as e:  # the checker leg must not hide the GPU line
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+            "warmup": args.warmup, "ms_per_step": t_max / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded jittered fluid block, lattice body; no dataset in the reference)",
+            "config": {"workload": "gpu_default: 20^3 body (8,000 particles, 93,556 constraints) + 65,536 "
+                                   "fluid, 30 mm radius, T=2^18, 5 substeps x 3 Jacobi iterations per "
+                                   "frame (dt=1/60), slice wedge at frame 60",
+                       "frames": K, "particles": active, "substeps": sc.substeps,
+                       "solid_iters": sc.desc.solid_iters, "l2": "flushed between frames (256 MB write)",
+                       "parallelism": f"replicas x{ws}", "graphs": True},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(info.param_bytes),
+                    "d2h_bytes_per_step": int(info.total * 16 + info.total * 4), "frames": E,
+                    "path": "upbd_step + upbd_read_state(pos, flags) into pinned host memory"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,396 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracles.
+
+Integer work is bit-exact against O1, the restatement of the CPU solver
+(src/solver.js): hash-grid counts, offsets and per-bucket membership, the
+alive flags a slice wedge leaves, and pick results. Every floating-point pass
+is bit-exact against O2<float> (the WGSL kernels restated) in the
+--fmad=false parity build, and within the stated per-substep tolerance in the
+FMA product build.
+"""
+import numpy as np
+import pytest
+
+from fluidphysics_b200 import _lib as L
+from fluidphysics_b200 import scenes as S
+from fluidphysics_b200.sim import Sim, sim_from_scene
+from helpers import (assert_states_close, assert_states_equal, load_state, settled_state)
+from oracle.oracle import o1_from_scene, o2_from_scene
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c1_settled():
+    sc = S.cpu_scene()
+    o2, st, cons = settled_state(sc, 25)
+    return sc, st, cons
+
+
+@pytest.fixture(scope="module")
+def c2_settled():
+    sc = S.gpu_default(frames=1)
+    o2, st, cons = settled_state(sc, 4)
+    return sc, st, cons
+
+
+def o1_grid_for(scene, pos3, active):
+    o1 = o1_from_scene(scene)
+    o1.set("pos", pos3.astype(np.float32).reshape(-1))
+    o1.set("active", active.astype(np.uint8))
+    o1.run_pass("grid")
+    return o1.get("cellStart").astype(np.uint32), o1.get("cellEntries").astype(np.uint32)
+
+
+# ------------------------------------------------------------------ grid
+@pytest.mark.parametrize("which", ["c1_init", "c1_settled", "c2_init", "c2_settled"])
+def test_grid_bit_exact_vs_cpu_solver(which, request):
+    if which.endswith("init"):
+        sc = S.cpu_scene() if which.startswith("c1") else S.gpu_default(frames=1)
+        sim = sim_from_scene(sc)
+    else:
+        sc, st, cons = request.getfixturevalue(which.replace("_settled", "_settled"))
+        sim = sim_from_scene(sc)
+        load_state(sim, st, cons)
+    sim.rebuild_grid()
+    counts, offs, ent = sim.read_grid()
+    g = sim.read_state()
+    cs, ce = o1_grid_for(sc, g["pos"][:, :3], g["flags"] & 1)
+    assert np.array_equal(offs, cs)
+    assert np.array_equal(ent, ce[: offs[-1]])
+    assert np.array_equal(counts, np.diff(cs))
+
+
+def test_grid_edge_positions():
+    """Cell boundaries, negative and huge coordinates, non-finite values:
+    the GPU hash follows JavaScript's Math.floor / ToInt32 semantics."""
+    sc = S.cpu_scene()
+    sim = sim_from_scene(sc)
+    n = sim.info.total
+    rng = np.random.default_rng(11)
+    cs = 0.22
+    k = rng.integers(-400, 400, size=(n, 3)).astype(np.float64)
+    pos = (k * cs).astype(np.float32)                      # exactly on boundaries (as float32)
+    pos[::7] = np.nextafter(pos[::7], np.float32(-np.inf))  # just below
+    pos[::11] = rng.uniform(-1e6, 1e6, size=pos[::11].shape).astype(np.float32)
+    pos[::13] = rng.uniform(-1e9, 1e9, size=pos[::13].shape).astype(np.float32)
+    pos[5] = [np.nan, 1.0, 2.0]
+    pos[6] = [np.inf, -np.inf, 0.0]
+    p4 = np.zeros((n, 4), np.float32)
+    p4[:, :3] = pos
+    flags = np.ones(n, np.uint32)
+    sim.write_state(pos=p4, flags=flags)
+    sim.rebuild_grid()
+    counts, offs, ent = sim.read_grid()
+    cs_ref, ce_ref = o1_grid_for(sc, pos, flags)
+    assert np.array_equal(offs, cs_ref)
+    assert np.array_equal(ent, ce_ref[: offs[-1]])
+
+
+def test_stateless_grid_build_matches():
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    sc = S.gpu_default(frames=1)
+    o1 = o1_from_scene(sc)
+    pos = o1.get("pos").reshape(-1, 3)
+    act = o1.get("active")
+    n = pos.shape[0]
+    T = sc.desc.table_size
+    p4 = np.zeros((n, 4), np.float32)
+    p4[:, :3] = pos
+    dev = torch.device("cuda:0")
+    d_pos = torch.from_numpy(p4).to(dev)
+    d_flags = torch.from_numpy(act.astype(np.int32)).to(dev)
+    d_off = torch.zeros(T + 1, dtype=torch.int32, device=dev)
+    d_ent = torch.zeros(n, dtype=torch.int32, device=dev)
+    d_cnt = torch.zeros(T, dtype=torch.int32, device=dev)
+    lib = L.load()
+    for _ in range(2):  # the scratch pool is reused across calls
+        rc = lib.upbd_grid_build(C.c_void_p(d_pos.data_ptr()), C.c_void_p(d_flags.data_ptr()), n, T,
+                                 sc.params.cell_size, C.c_void_p(d_cnt.data_ptr()),
+                                 C.c_void_p(d_off.data_ptr()), C.c_void_p(d_ent.data_ptr()),
+                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0, lib.upbd_last_error(None)
+        torch.cuda.synchronize()
+        o1.run_pass("grid")
+        cs = o1.get("cellStart").astype(np.uint32)
+        ce = o1.get("cellEntries").astype(np.uint32)
+        assert np.array_equal(d_off.cpu().numpy().view(np.uint32), cs)
+        assert np.array_equal(d_ent.cpu().numpy().view(np.uint32)[: cs[-1]], ce[: cs[-1]])
+        assert np.array_equal(d_cnt.cpu().numpy().view(np.uint32), np.diff(cs))
+
+
+# ------------------------------------------------------------------ cut / pick
+def wedges(center, n, seed):
+    return [S.wedge_through(np.asarray(center) + np.random.default_rng(seed + k).normal(size=3) * 0.1,
+                            seed + k) for k in range(n)]
+
+
+@pytest.mark.parametrize("which", ["c2_init", "c2_settled", "c1_settled"])
+def test_slice_alive_flags_bit_exact_vs_cpu_solver(which, request):
+    if which == "c2_init":
+        sc = S.gpu_default(frames=1)
+        sim = sim_from_scene(sc)
+    else:
+        sc, st, cons = request.getfixturevalue(which)
+        sim = sim_from_scene(sc)
+        load_state(sim, st, cons)
+    g = sim.read_state()
+    o1 = o1_from_scene(sc)
+    o1.set("pos", g["pos"][:, :3].reshape(-1))
+    cons0 = sim.read_constraints()
+    o1.set("consAlive", cons0[:, 3].astype(np.uint8))
+    total = 0
+    for o, d1, d2 in [sc.wedge or wedges(sc.desc.cube_center, 1, 5)[0]] + wedges(sc.desc.cube_center, 6, 17):
+        n_gpu = sim.slice_now(o, d1, d2)
+        n_cpu = o1.cut(o, d1, d2)
+        assert n_gpu == n_cpu
+        total += n_gpu
+        assert np.array_equal(sim.read_constraints()[:, 3], o1.get("consAlive").astype(np.uint32))
+    assert total > 0
+
+
+def test_queued_slice_applies_after_frame():
+    sc = S.gpu_default(frames=1)
+    sim = sim_from_scene(sc, "parity")
+    o2 = o2_from_scene(sc)
+    o, d1, d2 = sc.wedge
+    sim.slice(o, d1, d2)
+    o2.slice(o, d1, d2)
+    sim.step(sc.dt, sc.substeps)
+    o2.step(sc.dt, sc.substeps)
+    c_gpu = sim.read_constraints()
+    c_cpu, _ = o2.read_constraints()
+    assert np.array_equal(c_gpu, c_cpu)
+    assert c_gpu[:, 3].sum() < sim.info.num_cons
+
+
+def test_pick_exact_vs_cpu_solver(c2_settled):
+    sc, st, cons = c2_settled
+    sim = sim_from_scene(sc)
+    load_state(sim, st, cons)
+    o1 = o1_from_scene(sc)
+    o1.set("pos", sim.read_state()["pos"][:, :3].reshape(-1))
+    rng = np.random.default_rng(3)
+    c = np.array(sc.desc.cube_center)
+    hits = 0
+    for _ in range(40):
+        ro = c + rng.normal(size=3) * 4
+        rd = (c + rng.normal(size=3) * 0.4) - ro
+        rd /= np.linalg.norm(rd)
+        gi, gt = sim.pick(ro, rd, 0.25)
+        ci, ct = o1.pick(ro, rd, 0.25)
+        assert gi == ci and (gi < 0 or gt == ct)
+        hits += gi >= 0
+    assert hits > 10
+
+
+# ------------------------------------------------------------------ passes
+PASSES = ["INTEGRATE", "GRID", "DENSITY", "DISP", "APPLY_FLUID", "SOLID", "BONDS", "CONTACTS",
+          "APPLY_ALL", "BOUNDS", "VELOCITY", "XSPH", "XSPH_APPLY"]
+
+
+@pytest.mark.parametrize("which", ["c1_settled", "c2_settled"])
+@pytest.mark.parametrize("pass_name", PASSES)
+def test_pass_bit_exact_parity_build(which, pass_name, request):
+    sc, st, cons = request.getfixturevalue(which)
+    sim = sim_from_scene(sc, "parity")
+    load_state(sim, st, cons)
+    o2 = o2_from_scene(sc)
+    o2.write_state(**st)
+    o2.write_constraints(cons)
+    h = sc.dt / sc.substeps
+    last = L.PASS[pass_name]
+    sim.substep_partial(h, last)
+    o2.substep_partial(h, last)
+    assert_states_equal(sim.read_state(), o2.read_state(), pass_name)
+    assert np.array_equal(sim.read_constraints(), o2.read_constraints()[0])
+    if last >= L.PASS["GRID"]:
+        c_g, o_g, e_g = sim.read_grid()
+        c_o, o_o, e_o = o2.read_grid()
+        assert np.array_equal(o_g, o_o) and np.array_equal(e_g, e_o)
+
+
+@pytest.mark.parametrize("which", ["c1_settled", "c2_settled"])
+def test_substeps_within_tolerance_product_build(which, request):
+    sc, st, cons = request.getfixturevalue(which)
+    sim = sim_from_scene(sc, "product")
+    load_state(sim, st, cons)
+    o2 = o2_from_scene(sc)
+    o2.write_state(**st)
+    o2.write_constraints(cons)
+    h = sc.dt / sc.substeps
+    errs = []
+    for k in range(3):  # each substep from an identical state
+        sim.substep_partial(h, 1000)
+        o2.substep_partial(h, 1000)
+        g, r = sim.read_state(), o2.read_state()
+        errs.append(assert_states_close(g, r, f"substep {k}"))
+        load_state(sim, r, o2.read_constraints()[0])
+    print(which, errs)
+
+
+def test_frame_parity_build_bit_exact(c1_settled):
+    sc, st, cons = c1_settled
+    sim = sim_from_scene(sc, "parity")
+    load_state(sim, st, cons)
+    o2 = o2_from_scene(sc)
+    o2.write_state(**st)
+    o2.write_constraints(cons)
+    for _ in range(3):
+        sim.step(sc.dt, sc.substeps)
+        o2.step(sc.dt, sc.substeps)
+    assert_states_equal(sim.read_state(), o2.read_state(), "3 frames")
+    assert np.array_equal(sim.read_constraints(), o2.read_constraints()[0])
+
+
+@pytest.mark.parametrize("features", [L.FEAT_TETS, L.FEAT_SOLID_CONTACTS,
+                                      L.FEAT_TETS | L.FEAT_SOLID_CONTACTS])
+def test_optional_passes_bit_exact(features):
+    """Tet volume constraints and the solid contact cache (the GPU
+    reference's full schedule, src/gpu/sim.js:365-375), with the companion
+    cube of src/gpu/sim.js:83."""
+    d, p, opts = S.gpu_scene(10, 4096, 40, iters=3, features=features)
+    d.solid_dim2 = 4
+    d.cube2_center[:] = [0.25, 0.5 + 3 * d.spacing / 2 + 1.0, 0.1]
+    fp = S.jittered_block(16, 16, 16, 2.2 * 0.04, 1.9, 9)
+    sc = S.Scene("feat", d, p, fp, np.zeros_like(fp), opts["fluidMass"], 1 / 60, 5, 10)
+    sim = sim_from_scene(sc, "parity")
+    o2 = o2_from_scene(sc)
+    for f in range(8):
+        sim.step(sc.dt, sc.substeps)
+        o2.step(sc.dt, sc.substeps)
+    assert_states_equal(sim.read_state(), o2.read_state(), f"features {features}")
+    assert np.array_equal(sim.read_constraints(), o2.read_constraints()[0])
+    assert np.array_equal(sim.read_tets(), o2.read_tets())
+
+
+# ------------------------------------------------------------------ tools
+def test_grab_select_and_move_parity_build(c1_settled):
+    sc, st, cons = c1_settled
+    sim = sim_from_scene(sc, "parity")
+    load_state(sim, st, cons)
+    o2 = o2_from_scene(sc)
+    o2.write_state(**st)
+    o2.write_constraints(cons)
+    top = st["pos"][:343, :3][np.argmax(st["pos"][:343, 1])]
+    for s_ in (sim, o2):
+        s_.grab_select(top, 0.45)
+    assert_states_equal(sim.read_state(), o2.read_state(), "grab select")
+    for f in range(4):
+        for s_ in (sim, o2):
+            s_.grab_move((0.01, 0.05, 0.0))
+            s_.step(sc.dt, sc.substeps)
+    assert_states_equal(sim.read_state(), o2.read_state(), "grab move")
+    for s_ in (sim, o2):
+        s_.release()
+    assert_states_equal(sim.read_state(), o2.read_state(), "release")
+
+
+def test_grab_indices_with_targets_parity_build(c1_settled):
+    sc, st, cons = c1_settled
+    sim = sim_from_scene(sc, "parity")
+    load_state(sim, st, cons)
+    o2 = o2_from_scene(sc)
+    o2.write_state(**st)
+    o2.write_constraints(cons)
+    idx = np.arange(0, 343, 7, dtype=np.uint32)
+    tg = st["pos"][idx, :3].astype(np.float32) + np.float32(0.2)
+    w = np.linspace(0.1, 1.0, idx.size).astype(np.float32)
+    sim.grab_indices(idx, w, tg)
+    o2.grab_indices(idx, w, tg)
+    for _ in range(2):
+        sim.step(sc.dt, sc.substeps)
+        o2.step(sc.dt, sc.substeps)
+    assert_states_equal(sim.read_state(), o2.read_state(), "grab indices")
+
+
+def test_emit_hose_matches_oracle():
+    sc = S.cpu_scene()
+    sim = sim_from_scene(sc, "parity")
+    o2 = o2_from_scene(sc)
+    args = ((0.0, 3.0, 0.0), (0.6, -0.8, 0.0), (0.0, 0.0, 1.0), (0.8, 0.6, 0.0), 7.5, 1.234)
+    for s_ in (sim, o2):
+        s_.emit(200, *args)
+    h = sc.dt / sc.substeps
+    sim.step(h, 1)  # emit runs at the start of the frame
+    o2.step(h, 1)
+    g, r = sim.read_state(), o2.read_state()
+    assert np.array_equal(g["flags"], r["flags"])
+    assert sim.get_info().fluid_next == o2.fluid_next() == 200
+    # emit evaluates sin/cos (CUDA vs the C library): positions agree to a few
+    # ulps, the fract(sin(x)*43758) jitter to 1e-2 m/s
+    slots = slice(343, 343 + 200)
+    assert np.abs(g["pos"][slots, :3] - r["pos"][slots, :3]).max() < 1e-4
+    assert np.abs(g["vel"][slots, :3] - r["vel"][slots, :3]).max() < 2e-2
+
+
+def test_drain_count_reset():
+    sc = S.cpu_scene()
+    sim = sim_from_scene(sc)
+    assert sim.active_count() == 2600
+    sim.step(sc.dt, sc.substeps)
+    sim.drain()
+    assert sim.active_count() == 0
+    sim.emit_particles(sc.fluid_pos[:100], sc.fluid_vel[:100], sc.fluid_mass)
+    assert sim.active_count() == 100
+    sim.reset_solid()
+    st = sim.read_state()
+    assert np.all(st["vel"] == 0) and np.all(st["flags"][:343] == 1)
+    assert np.array_equal(sim.read_constraints()[:, 3], np.ones(sim.info.num_cons, np.uint32))
+
+
+def test_graph_and_eager_frames_identical():
+    sc = S.cpu_scene()
+    a = sim_from_scene(sc)
+    b = sim_from_scene(sc)
+    b.set_graphs(False)
+    o, d1, d2 = S.wedge_through(sc.desc.cube_center, 4)
+    for f in range(6):
+        if f == 3:
+            a.slice(o, d1, d2)
+            b.slice(o, d1, d2)
+        a.step(sc.dt, sc.substeps)
+        b.step(sc.dt, sc.substeps)
+    sa, sb = a.read_state(), b.read_state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+    assert np.array_equal(a.read_constraints(), b.read_constraints())
+    assert a.launches > 0
+
+
+def test_nan_state_reported_by_sync():
+    """Failure detection without a GPU fault: a non-finite velocity written
+    from the host makes the step's check set the NaN health bit, and
+    upbd_sync reports UPBD_ERR_NAN; the context stays usable."""
+    sc = S.cpu_scene()
+    sim = sim_from_scene(sc)
+    st = sim.read_state()
+    st["pos"][400, 0] = np.nan
+    sim.write_state(pos=st["pos"])
+    sim.step(sc.dt, sc.substeps)
+    with pytest.raises(L.UpbdError, match="NAN"):
+        sim.sync()
+    assert sim.health() & L.HEALTH_NAN
+    sim.clear_health()
+    sim.reset_solid()
+    sim.drain()
+    sim.step(sc.dt, sc.substeps)
+    sim.sync()
+
+
+def test_invalid_arguments_rejected():
+    sc = S.cpu_scene()
+    sim = sim_from_scene(sc)
+    with pytest.raises(L.UpbdError, match="INVALID"):
+        sim.grab_indices([5000])
+    with pytest.raises(L.UpbdError, match="INVALID"):
+        sim.grab_indices([3, 3])
+    with pytest.raises(L.UpbdError, match="CAPACITY"):
+        sim.emit(10 ** 6, (0, 0, 0), (0, 1, 0), (1, 0, 0), (0, 0, 1), 1.0, 0.0)
+    with pytest.raises(L.UpbdError, match="INVALID"):
+        sim.step(1 / 60, 0)
+    d = L.SceneDesc()
+    S._fill_default_desc(d)
+    d.table_size = 1000
+    with pytest.raises(L.UpbdError, match="INVALID"):
+        Sim(d, S.default_params())
