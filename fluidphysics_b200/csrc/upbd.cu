@@ -183,6 +183,10 @@ void fill_static_params(upbd_sim* s) {
   d.inv_cell = 1.0 / p.cell_size;  // Solver._hashPos: 1 / cellSize in double
   d.tear_mode = p.tear_mode;
   d.plastic_clamp = p.plastic_clamp;
+  // solid↔fluid contacts only within adjacent cells: the marking shortcut is
+  // exact (the marked set only grows by the 1e-5 slack of mark_fluid_near)
+  const double rsum = (double)(d.solid_radius + d.fluid_radius);
+  d.use_mark = (rsum * 1.0001 < p.cell_size * (1.0 - 1e-6)) ? 1 : 0;
 }
 
 int upload_params(upbd_sim* s) {
@@ -220,10 +224,11 @@ int launch_substep(upbd_sim* s, int last) {
   L += 4;
   UPBD_KCK(s);
   if (last < UPBD_PASS_DENSITY) return UPBD_OK;
-  PROF(s, K_DENSITY, k_density<<<blocks_for(v.F), 256, 0, st>>>(v, P));
+  const long long fl = (long long)v.F * GL;  // lane-parallel fluid gathers
+  PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_DISP) return UPBD_OK;
-  PROF(s, K_DISP, k_disp<<<blocks_for(v.F), 256, 0, st>>>(v, P));
+  PROF(s, K_DISP, k_disp<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   UPBD_KCK(s);
   if (last < UPBD_PASS_APPLY_FLUID) return UPBD_OK;
@@ -236,12 +241,20 @@ int launch_substep(upbd_sim* s, int last) {
     PROF(s, K_COLLECT, k_collect_contacts<<<blocks_for(v.S), 256, 0, st>>>(v, P));
     L++;
   }
+  // the contact marks ride on the last applyDeltaSolid when that is the last
+  // position update of the solve; otherwise they get their own launch
+  const bool mark_in_apply = iters > 0 && !tets && !scc;
+  const int solid_pad = ((v.S * GL + 31) / 32) * 32;  // lane threads of the solve, whole warps
   for (int it = 0; it < iters; it++) {
     if (it == 0)
-      PROF(s, K_SOLID_SOLVE, k_solid_solve<true><<<blocks_for(v.N), 256, 0, st>>>(v, P));
+      PROF(s, K_SOLID_SOLVE,
+           k_solid_solve<true><<<blocks_for((long long)solid_pad + v.F), 256, 0, st>>>(v, P, solid_pad));
     else
-      PROF(s, K_SOLID_SOLVE, k_solid_solve<false><<<blocks_for(v.S), 256, 0, st>>>(v, P));
-    PROF(s, K_APPLY_SOLID, k_apply_solid<<<blocks_for(v.S), 256, 0, st>>>(v, P));
+      PROF(s, K_SOLID_SOLVE, k_solid_solve<false><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad));
+    if (mark_in_apply && it == iters - 1)
+      PROF(s, K_APPLY_SOLID, k_apply_solid<true><<<blocks_for((long long)v.S * GL), 256, 0, st>>>(v, P));
+    else
+      PROF(s, K_APPLY_SOLID, k_apply_solid<false><<<blocks_for(v.S), 256, 0, st>>>(v, P));
     L += 2;
     if (tets) {
       PROF(s, K_SOLVE_TETS, k_solve_tets<<<blocks_for(v.S), 256, 0, st>>>(v, P));
@@ -254,12 +267,19 @@ int launch_substep(upbd_sim* s, int last) {
       L += 2;
     }
   }
+  if (!mark_in_apply && v.S > 0) {
+    PROF(s, K_APPLY_SOLID, k_contact_mark<<<blocks_for((long long)v.S * GL), 256, 0, st>>>(v, P));
+    L++;
+  }
   UPBD_KCK(s);
   if (last < UPBD_PASS_BONDS) return UPBD_OK;
   {
     const int nb = v.C, nt = tets ? v.NT : 0;
+    const int nb_pad = ((nb + nt + 31) / 32) * 32;
     const int nc = (last < UPBD_PASS_CONTACTS) ? 0 : v.N;
-    PROF(s, K_BOND_CONTACTS, k_bond_contacts<<<blocks_for((long long)nb + nt + nc), 256, 0, st>>>(v, P, nb, nt, nc));
+    const long long threads = (long long)nb_pad + (long long)nc * GL;
+    PROF(s, K_BOND_CONTACTS,
+         k_bond_contacts<<<blocks_for(threads), 256, 0, st>>>(v, P, nb, nt, nb_pad, nc));
     L++;
   }
   if (last < UPBD_PASS_APPLY_ALL) return UPBD_OK;
@@ -276,7 +296,7 @@ int launch_substep(upbd_sim* s, int last) {
     L += 2;
   }
   if (last < UPBD_PASS_XSPH) return UPBD_OK;
-  PROF(s, K_XSPH, k_xsph<<<blocks_for(v.F), 256, 0, st>>>(v, P));
+  PROF(s, K_XSPH, k_xsph<<<blocks_for((long long)v.F * GL), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_XSPH_APPLY) return UPBD_OK;
   PROF(s, K_XSPH_APPLY, k_xsph_apply<<<blocks_for(v.F), 256, 0, st>>>(v));
@@ -403,6 +423,8 @@ struct HostScene {
   std::vector<float4> pos;
   std::vector<uint4> cons;
   std::vector<uint32_t> adj;
+  std::vector<uint32_t> adj_other;
+  std::vector<float> adj_scale;
   std::vector<uint32_t> tet_idx;
   std::vector<float> tet_vol;
   std::vector<uint32_t> tet_adj;
@@ -505,6 +527,21 @@ void build_scene(const upbd_scene_desc& d, HostScene& out) {
     for (uint32_t c : inc[i]) out.adj[out.S + 1 + off++] = c;
   }
   out.adj[out.S] = off;
+  // CSR-parallel static data of the Jacobi gather: the other endpoint of each
+  // incident constraint and the pair scale 1/max(deg_i, deg_j) of
+  // src/gpu/wgsl.js:340-354 (endpoints and degrees never change)
+  out.adj_other.assign(2 * (size_t)C, 0);
+  out.adj_scale.assign(2 * (size_t)C, 0.f);
+  for (int i = 0; i < out.S; i++) {
+    const uint32_t degI = out.adj[i + 1] - out.adj[i];
+    for (uint32_t k = out.adj[i]; k < out.adj[i + 1]; k++) {
+      const uint32_t c = out.adj[out.S + 1 + k];
+      const uint32_t other = (ca[c] == (uint32_t)i) ? cb[c] : ca[c];
+      const uint32_t degJ = out.adj[other + 1] - out.adj[other];
+      out.adj_other[k] = other;
+      out.adj_scale[k] = 1.0f / (float)((degI < degJ) ? degJ : degI);
+    }
+  }
   const int NT = (int)out.tet_vol.size();
   std::vector<std::vector<uint32_t>> tinc(out.S);
   for (int t = 0; t < NT; t++)
@@ -633,6 +670,14 @@ int upbd_create(const upbd_scene_desc* desc, const upbd_params* params, upbd_sim
   const size_t o_tvol = cv.take<float>(std::max(v.NT, 1));
   const size_t o_tadj = cv.take<uint32_t>(hs.tet_adj.size());
   const bool scc = (desc->features & UPBD_FEAT_SOLID_CONTACTS) != 0;
+  const size_t o_mark = cv.take<uint32_t>(v.N);
+  const size_t o_spos = cv.take<float4>(v.N), o_sdens = cv.take<float2>(v.N), o_svel = cv.take<float4>(v.N);
+  const size_t o_slot = cv.take<uint32_t>(v.N);
+  const size_t o_fend = cv.take<uint32_t>(v.T);
+  const size_t o_nbr = cv.take<uint32_t>(std::max<size_t>((size_t)v.F * GL * NL, 1));
+  const size_t o_ncount = cv.take<uint32_t>(std::max<size_t>((size_t)v.F * GL, 1));
+  const size_t o_aoth = cv.take<uint32_t>(std::max<size_t>(hs.adj_other.size(), 1));
+  const size_t o_ascl = cv.take<float>(std::max<size_t>(hs.adj_scale.size(), 1));
   const size_t o_ccount = cv.take<uint32_t>(scc ? std::max(v.S, 1) : 1);
   const size_t o_clist = cv.take<uint32_t>(scc ? (size_t)std::max(v.S, 1) * C_K : 1);
   const size_t o_scr = cv.take<uint32_t>(SCR_WORDS);
@@ -661,6 +706,16 @@ int upbd_create(const upbd_scene_desc* desc, const upbd_params* params, upbd_sim
   v.tet_idx = (uint32_t*)(base + o_tidx);
   v.tet_vol = (float*)(base + o_tvol);
   v.tet_adj = (const uint32_t*)(base + o_tadj);
+  v.mark = (uint32_t*)(base + o_mark);
+  v.spos = (float4*)(base + o_spos);
+  v.sdens = (float2*)(base + o_sdens);
+  v.svel = (float4*)(base + o_svel);
+  v.slot = (uint32_t*)(base + o_slot);
+  v.fend = (uint32_t*)(base + o_fend);
+  v.nbr = (uint32_t*)(base + o_nbr);
+  v.ncount = (uint32_t*)(base + o_ncount);
+  v.adj_other = (const uint32_t*)(base + o_aoth);
+  v.adj_scale = (const float*)(base + o_ascl);
   v.ccount = (uint32_t*)(base + o_ccount);
   v.clist = (uint32_t*)(base + o_clist);
   v.scratch = (uint32_t*)(base + o_scr);
@@ -690,6 +745,12 @@ int upbd_create(const upbd_scene_desc* desc, const upbd_params* params, upbd_sim
   cudaStream_t st = s->stream;
   bool ok = cudaMemsetAsync(s->arena, 0, s->arena_bytes, st) == cudaSuccess;
   ok = ok && cudaMemcpyAsync((void*)v.adj, hs.adj.data(), hs.adj.size() * 4, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  if (!hs.adj_other.empty()) {
+    ok = ok && cudaMemcpyAsync((void*)v.adj_other, hs.adj_other.data(), hs.adj_other.size() * 4,
+                               cudaMemcpyHostToDevice, st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync((void*)v.adj_scale, hs.adj_scale.data(), hs.adj_scale.size() * 4,
+                               cudaMemcpyHostToDevice, st) == cudaSuccess;
+  }
   if (!hs.tet_adj.empty())
     ok = ok && cudaMemcpyAsync((void*)v.tet_adj, hs.tet_adj.data(), hs.tet_adj.size() * 4, cudaMemcpyHostToDevice, st) == cudaSuccess;
   if (!hs.tet_idx.empty())

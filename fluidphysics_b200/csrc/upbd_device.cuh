@@ -50,6 +50,10 @@ struct DevParams {
   float contact_scale, pad0, pad1, pad2;
   double inv_cell;
   int32_t tear_mode, plastic_clamp;
+  // 1 when solid_radius + fluid_radius is below the cell size: every
+  // solid↔fluid contact then lies in adjacent cells, so the solids can mark
+  // the fluid particles that have one and the rest skip their gather.
+  int32_t use_mark, pad4;
   float4 grab_delta;  // per-substep share of the frame's grab motion
   uint32_t emit_count, emit_start, grab_lattice, pad3;
   float4 emit_pos, emit_dir, emit_side, emit_up;
@@ -78,6 +82,25 @@ struct SimView {
   uint32_t* tet_idx;   // 4 per tet
   float* tet_vol;      // rest volume, negative = dead
   const uint32_t* tet_adj;  // [S+1 offsets][4NT ids]
+  // Bucket-ordered copies, slot e matching entries[e]: neighbour gathers read
+  // a candidate's data with one load at its slot instead of entries -> pos.
+  // Every pass that moves a particle also writes its slot's copy.
+  float4* spos;        // position + inverse mass
+  float2* sdens;       // (rho, rho_near) of the density pass
+  float4* svel;        // velocity after velocityUpdate
+  uint32_t* slot;      // slot of particle i in this substep's grid
+  // Inside a bucket, entries run in descending index, so fluid (indices >= S)
+  // precede solids: fend[h] splits bucket h into [start[h], fend[h]) fluid and
+  // [fend[h], start[h+1]) solid.
+  uint32_t* fend;
+  // Density-pass neighbour lists: lane g = (i - S)*GL + l of fluid particle i
+  // records the slots of its in-range fluid neighbours, in walk order, at
+  // nbr[c * F*GL + g] (c < NL), and their number in ncount[g].
+  uint32_t* nbr;
+  uint32_t* ncount;
+  const uint32_t* adj_other;  // CSR-parallel: the other endpoint of constraint ids[k]
+  const float* adj_scale;     // CSR-parallel: 1 / max(deg_i, deg_other) (static)
+  uint32_t* mark;      // per particle: a solid is within contact range (fluid only)
   uint32_t* ccount;
   uint32_t* clist;
   uint32_t* scratch;
@@ -117,7 +140,95 @@ struct CellHash {
   __device__ __forceinline__ uint32_t bucket(int a, int b, int c, uint32_t mask) const {
     return (uint32_t)(hx[a] ^ hy[b] ^ hz[c]) & mask;
   }
+  // Bucket of neighbour cell k = (dx+1)*9 + (dy+1)*3 + (dz+1) with a runtime
+  // k: selects keep the nine hashes in registers.
+  __device__ __forceinline__ uint32_t bucket_k(int k, uint32_t mask) const {
+    const int a = k / 9, r = k - 9 * a, b = r / 3, c = r - 3 * b;
+    const int32_t X = (a == 0) ? hx[0] : ((a == 1) ? hx[1] : hx[2]);
+    const int32_t Y = (b == 0) ? hy[0] : ((b == 1) ? hy[1] : hy[2]);
+    const int32_t Z = (c == 0) ? hz[0] : ((c == 1) ? hz[1] : hz[2]);
+    return (uint32_t)(X ^ Y ^ Z) & mask;
+  }
 };
+
+// Neighbour gathers run GL lanes per particle: lane l walks the neighbour
+// cells k = l, l+GL, l+2GL, l+3GL (k < 27, in the reference's dx/dy/dz order)
+// and each bucket's entries in order, accumulating its own partial sums from
+// zero; the GL partials are then combined by a fixed xor butterfly, so the
+// result is deterministic: ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
+constexpr int GL = 8;
+constexpr uint32_t NL = 16;  // neighbour-list entries kept per lane
+
+__device__ __forceinline__ float lane_sum(float x) {
+  x = x + __shfl_xor_sync(0xffffffffu, x, 4);
+  x = x + __shfl_xor_sync(0xffffffffu, x, 2);
+  x = x + __shfl_xor_sync(0xffffffffu, x, 1);
+  return x;
+}
+
+// The nine hash components of the cells around p (CellHash::init's values),
+// computed two per lane of a GL group and exchanged by shuffles. Every lane of
+// the warp must call it (inactive groups pass any position).
+__device__ __forceinline__ void group_cell_hash(float px, float py, float pz, double inv, CellHash& ch) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & (GL - 1);
+  const int base = (threadIdx.x & 31) & ~(GL - 1);
+  // lane l holds component l: x offsets -1..1 (lanes 0-2), y (3-5), z -1, 0 (6-7)
+  const int axis = lane / 3;
+  const float pa = (axis == 0) ? px : ((axis == 1) ? py : pz);
+  const double K = (axis == 0) ? 92837111.0 : ((axis == 1) ? 689287499.0 : 283923481.0);
+  const double c = floor(__dmul_rn((double)pa, inv));
+  const int32_t v1 = js_toint32(__dmul_rn(__dadd_rn(c, (double)(lane - 3 * axis - 1)), K));
+  // z offset +1, taken from the group's first lane
+  const double cz = floor(__dmul_rn((double)pz, inv));
+  const int32_t v2 = js_toint32(__dmul_rn(__dadd_rn(cz, 1.0), 283923481.0));
+  ch.hx[0] = __shfl_sync(FULL, v1, base + 0);
+  ch.hx[1] = __shfl_sync(FULL, v1, base + 1);
+  ch.hx[2] = __shfl_sync(FULL, v1, base + 2);
+  ch.hy[0] = __shfl_sync(FULL, v1, base + 3);
+  ch.hy[1] = __shfl_sync(FULL, v1, base + 4);
+  ch.hy[2] = __shfl_sync(FULL, v1, base + 5);
+  ch.hz[0] = __shfl_sync(FULL, v1, base + 6);
+  ch.hz[1] = __shfl_sync(FULL, v1, base + 7);
+  ch.hz[2] = __shfl_sync(FULL, v2, base + 0);
+}
+
+// Walk this lane's neighbour cells: all bucket ranges are loaded first
+// (independent loads), then the candidates of the four buckets as one flat
+// sequence (bucket order, entries in order). PART 0 walks each bucket's fluid
+// entries, PART 1 its solid entries; fn(e) sees each slot e (the caller reads
+// the slot's bucket-ordered copies).
+template <int PART, class Fn>
+__device__ __forceinline__ void lane_slots(const SimView& v, const CellHash& ch, int lane, Fn&& fn) {
+  const uint32_t mask = (uint32_t)v.T - 1u;
+  uint32_t s[4], n[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const int k = lane + GL * m;
+    if (k < 27) {
+      const uint32_t hb = ch.bucket_k(k, mask);
+      const uint32_t f = __ldg(&v.fend[hb]);
+      if (PART == 0) {
+        s[m] = __ldg(&v.start[hb]);
+        n[m] = f - s[m];
+      } else {
+        s[m] = f;
+        n[m] = __ldg(&v.start[hb + 1]) - f;
+      }
+    } else {
+      s[m] = 0;
+      n[m] = 0;
+    }
+  }
+  const uint32_t n01 = n[0] + n[1], n012 = n01 + n[2], total = n012 + n[3];
+  for (uint32_t c = 0; c < total; c++) {
+    const uint32_t e = (c < n[0]) ? s[0] + c
+                     : (c < n01) ? s[1] + (c - n[0])
+                     : (c < n012) ? s[2] + (c - n01)
+                                  : s[3] + (c - n012);
+    fn(e);
+  }
+}
 
 __device__ __forceinline__ uint32_t cell_of(float px, float py, float pz, double inv, uint32_t mask) {
   const double cx = floor(__dmul_rn((double)px, inv));

@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(256) k_integrate_count(SimView v, const DevPar
     v.prev[i] = make_float4(px, py, pz, tw);
     p4 = make_float4(nx, ny, nz, p4.w);
     v.pos[i] = p4;
+    if (i >= v.S) v.mark[i] = 0u;  // contact marks of this substep start clear
   }
   if (COUNT) {
     const uint32_t h = cell_of(p4.x, p4.y, p4.z, P->inv_cell, (uint32_t)v.T - 1u);
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(SimView v) {
     const long long idx = t0 + k;
     if (idx < v.T) {
       v.start[idx] = run;
+      if (v.fend) v.fend[idx] = run;  // empty buckets; rankfix sets occupied ones
       v.counts[idx] = 0u;  // ready for the next count
     }
     run += c[k];
@@ -195,88 +197,127 @@ __global__ void __launch_bounds__(256) k_rankfix(SimView v) {
   if (!(v.flags[i] & F_ACTIVE)) return;
   const uint32_t h = v.cell[i];
   const uint32_t s = v.start[h], e = v.start[h + 1];
-  uint32_t rank = 0;
-  for (uint32_t k = s; k < e; k++) rank += (v.tmp[k] > (uint32_t)i) ? 1u : 0u;
+  uint32_t rank = 0, solids = 0;
+  for (uint32_t k = s; k < e; k++) {
+    const uint32_t j = v.tmp[k];
+    rank += (j > (uint32_t)i) ? 1u : 0u;
+    solids += (j < (uint32_t)v.S) ? 1u : 0u;
+  }
   v.entries[s + rank] = (uint32_t)i;
+  if (v.spos) {  // the stateless grid build has no bucket-ordered copies
+    v.slot[i] = s + rank;
+    v.spos[s + rank] = v.pos[i];
+    v.fend[h] = e - solids;  // every member writes the same value
+  }
 }
 
 // ------------------------------------------------------------------ fluid
+// The neighbour gathers run GL lanes per particle (see lane_slots): a warp
+// holds 32/GL particles, every lane reaches the shuffles, and lane 0 writes.
+
 // fluidDensity, src/gpu/wgsl.js:254-279
 __global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __restrict__ P) {
-  const int i = v.S + (int)UPBD_TID;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 pi = v.pos[i];
-  const float H = P->fluid_h, H2 = H * H;
-  const uint32_t mask = (uint32_t)v.T - 1u;
-  CellHash ch;
-  ch.init(pi.x, pi.y, pi.z, P->inv_cell);
+  const int t = UPBD_TID;
+  const int lane = threadIdx.x & (GL - 1);
+  const int i = v.S + t / GL;
+  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
   float rho = 0.f, rhoNear = 0.f;
-  for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++)
-      for (int c = 0; c < 3; c++) {
-        const uint32_t hb = ch.bucket(a, b, c, mask);
-        const uint32_t e1 = v.start[hb + 1];
-        for (uint32_t e = v.start[hb]; e < e1; e++) {
-          const uint32_t j = v.entries[e];
-          if (j == (uint32_t)i || j < (uint32_t)v.S) continue;
-          const float4 pj = v.pos[j];
-          const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-          const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-          if (d2 >= H2) continue;
-          const float q = 1.0f - sqrtf(d2) / H;
-          rho = rho + q * q;
-          rhoNear = rhoNear + q * q * q;
-        }
-      }
-  v.density[i] = make_float2(rho, rhoNear);
+  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  CellHash ch;
+  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
+  uint32_t myslot = 0;
+  if (act) {
+    const float H = P->fluid_h, H2 = H * H;
+    const float4* __restrict__ spos = v.spos;
+    myslot = v.slot[i];
+    const uint32_t FG = (uint32_t)v.F * GL;
+    const uint32_t g = (uint32_t)(i - v.S) * GL + lane;
+    uint32_t* __restrict__ nbr = v.nbr + g;
+    uint32_t cnt = 0;
+    lane_slots<0>(v, ch, lane, [&](uint32_t e) {
+      const float4 pj = spos[e];
+      if (e == myslot) return;
+      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      if (d2 >= H2) return;
+      const float q = 1.0f - sqrtf(d2) / H;
+      rho = rho + q * q;
+      rhoNear = rhoNear + q * q * q;
+      if (cnt < NL) nbr[cnt * FG] = e;  // for fluidDisp, same positions
+      cnt++;
+    });
+    v.ncount[g] = cnt;
+  }
+  rho = lane_sum(rho);
+  rhoNear = lane_sum(rhoNear);
+  if (act && lane == 0) {
+    const float2 d = make_float2(rho, rhoNear);
+    v.density[i] = d;
+    v.sdens[myslot] = d;
+  }
 }
 
 // fluidDisp, src/gpu/wgsl.js:281-316
 __global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __restrict__ P) {
-  const int i = v.S + (int)UPBD_TID;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 pi = v.pos[i];
+  const int t = UPBD_TID;
+  const int lane = threadIdx.x & (GL - 1);
+  const int i = v.S + t / GL;
+  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
   const float H = P->fluid_h, H2 = H * H;
-  const float maxPair = 0.05f * H, maxTotal = 0.35f * H;
-  const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
-  const float2 di = v.density[i];
-  const float Pi = k * (di.x - rho0);
-  const float PNi = kn * di.y;
-  const uint32_t mask = (uint32_t)v.T - 1u;
-  CellHash ch;
-  ch.init(pi.x, pi.y, pi.z, P->inv_cell);
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++)
-      for (int c = 0; c < 3; c++) {
-        const uint32_t hb = ch.bucket(a, b, c, mask);
-        const uint32_t e1 = v.start[hb + 1];
-        for (uint32_t e = v.start[hb]; e < e1; e++) {
-          const uint32_t j = v.entries[e];
-          if (j == (uint32_t)i || j < (uint32_t)v.S) continue;
-          const float4 pj = v.pos[j];
-          const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-          const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-          if (d2 >= H2 || d2 < 1e-12f) continue;
-          const float d = sqrtf(d2);
-          const float q = 1.0f - d / H;
-          const float2 dj = v.density[j];
-          const float Pj = k * (dj.x - rho0);
-          const float PNj = kn * dj.y;
-          float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
-          D = clampf(D, -maxPair, maxPair);
-          const float f = D / d;
-          sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
-        }
-      }
-  const float s2 = dot3(sx, sy, sz, sx, sy, sz);
-  if (s2 > maxTotal * maxTotal) {
-    const float f = maxTotal / sqrtf(s2);
-    sx = sx * f; sy = sy * f; sz = sz * f;
+  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t FG = (uint32_t)v.F * GL;
+  const uint32_t g = (uint32_t)(i - v.S) * GL + lane;
+  const uint32_t cnt = act ? v.ncount[g] : 0u;
+  CellHash ch;
+  if (__any_sync(0xffffffffu, cnt > NL)) group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
+  if (act) {
+    const float maxPair = 0.05f * H;
+    const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
+    const float2 di = v.density[i];
+    const float Pi = k * (di.x - rho0);
+    const float PNi = kn * di.y;
+    const float4* __restrict__ spos = v.spos;
+    const float2* __restrict__ sdens = v.sdens;
+    auto pair = [&](uint32_t e) {
+      const float4 pj = spos[e];
+      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      if (d2 >= H2 || d2 < 1e-12f) return;
+      const float d = sqrtf(d2);
+      const float q = 1.0f - d / H;
+      const float2 dj = sdens[e];
+      const float Pj = k * (dj.x - rho0);
+      const float PNj = kn * dj.y;
+      float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
+      D = clampf(D, -maxPair, maxPair);
+      const float f = D / d;
+      sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
+    };
+    // the density pass listed this lane's in-range neighbours at these same
+    // positions and in walk order; a lane whose list overflowed walks again
+    if (cnt <= NL) {
+      const uint32_t* __restrict__ nbr = v.nbr + g;
+      for (uint32_t c = 0; c < cnt; c++) pair(__ldg(&nbr[c * FG]));
+    } else {
+      const uint32_t myslot = v.slot[i];
+      lane_slots<0>(v, ch, lane, [&](uint32_t e) {
+        if (e != myslot) pair(e);
+      });
+    }
   }
-  v.delta[i] = make_float4(sx, sy, sz, 1.0f);
+  sx = lane_sum(sx);
+  sy = lane_sum(sy);
+  sz = lane_sum(sz);
+  if (act && lane == 0) {
+    const float maxTotal = 0.35f * H;
+    const float s2 = dot3(sx, sy, sz, sx, sy, sz);
+    if (s2 > maxTotal * maxTotal) {
+      const float f = maxTotal / sqrtf(s2);
+      sx = sx * f; sy = sy * f; sz = sz * f;
+    }
+    v.delta[i] = make_float4(sx, sy, sz, 1.0f);
+  }
 }
 
 // applyDeltaFluid, src/gpu/wgsl.js:318-323 (standalone form)
@@ -288,64 +329,127 @@ __global__ void k_apply_fluid(SimView v) {
   const float4 d = v.delta[i];
   p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
   v.pos[i] = p;
+  v.spos[v.slot[i]] = p;
 }
 
 // ------------------------------------------------------------------ solids
-// solidSolve, src/gpu/wgsl.js:326-359. With APPLY_FLUID the threads past the
-// solids apply the fluid displacement (applyDeltaFluid, src/gpu/wgsl.js:318-323):
-// the solve reads solid positions only, so the two passes share a launch.
+// solidSolve, src/gpu/wgsl.js:326-359, GL lanes per solid: lane l takes the
+// incident constraints k = st+l, st+l+GL, ... of the static CSR, whose other
+// endpoint and pair scale 1/max(deg_i, deg_j) are precomputed (both are fixed
+// for the life of the scene); the partials combine like lane_sum.
+// Threads from solid_pad on (a warp multiple, so the solve's warps are whole)
+// apply the fluid displacement when APPLY_FLUID (applyDeltaFluid,
+// src/gpu/wgsl.js:318-323): the solve reads solid positions only.
 template <bool APPLY_FLUID>
-__global__ void __launch_bounds__(256) k_solid_solve(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.S) {
+__global__ void __launch_bounds__(256) k_solid_solve(SimView v, const DevParams* __restrict__ P, int solid_pad) {
+  const int t = UPBD_TID;
+  if (t >= solid_pad) {
+    const int i = v.S + (t - solid_pad);
     if (APPLY_FLUID && i < v.N && (v.flags[i] & F_ACTIVE)) {
       float4 p = v.pos[i];
       const float4 d = v.delta[i];
       p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
       v.pos[i] = p;
+      v.spos[v.slot[i]] = p;
     }
     return;
   }
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 pi = v.pos[i];
-  const float wi = pi.w;
-  const float h = P->h;
-  const float alpha = P->compliance / (h * h);
-  const uint32_t st = v.adj[i], en = v.adj[i + 1];
-  const uint32_t degI = en - st;
-  const uint32_t* ids = v.adj + v.S + 1;
+  const int i = t / GL;
+  const int lane = threadIdx.x & (GL - 1);
+  const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
   float cx = 0.f, cy = 0.f, cz = 0.f;
-  for (uint32_t k = st; k < en; k++) {
-    const uint32_t ci = ids[k];
-    const uint4 c = v.cons[ci];
-    if (c.w == 0u) continue;
-    const uint32_t other = (c.x == (uint32_t)i) ? c.y : c.x;
-    const float rest = __uint_as_float(c.z);
-    const float4 po = v.pos[other];
-    const float ex = pi.x - po.x, ey = pi.y - po.y, ez = pi.z - po.z;
-    const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
-    if (d < 1e-9f) continue;
-    const float wsum = wi + po.w;
-    if (wsum == 0.f) continue;
-    const uint32_t degJ = v.adj[other + 1] - v.adj[other];
-    const float s = 1.0f / (float)((degI < degJ) ? degJ : degI);
-    const float dl = -(d - rest) / (wsum + alpha);
-    const float f = dl * wi / d * s;
-    cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
+  if (act) {
+    const float4 pi = v.pos[i];
+    const float wi = pi.w;
+    const float h = P->h;
+    const float alpha = P->compliance / (h * h);
+    const uint32_t st = v.adj[i], en = v.adj[i + 1];
+    const uint32_t* __restrict__ ids = v.adj + v.S + 1;
+    const uint4* __restrict__ cons = v.cons;
+    const float4* __restrict__ pos = v.pos;
+#pragma unroll 2
+    for (uint32_t k = st + lane; k < en; k += GL) {
+      const uint32_t ci = __ldg(&ids[k]);
+      const uint32_t other = __ldg(&v.adj_other[k]);
+      const float s = __ldg(&v.adj_scale[k]);
+      const float4 po = pos[other];
+      const uint2 rw = *reinterpret_cast<const uint2*>(&cons[ci].z);  // rest bits, alive
+      if (rw.y == 0u) continue;
+      const float rest = __uint_as_float(rw.x);
+      const float ex = pi.x - po.x, ey = pi.y - po.y, ez = pi.z - po.z;
+      const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
+      if (d < 1e-9f) continue;
+      const float wsum = wi + po.w;
+      if (wsum == 0.f) continue;
+      const float dl = -(d - rest) / (wsum + alpha);
+      const float f = dl * wi / d * s;
+      cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
+    }
   }
-  v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+  cx = lane_sum(cx);
+  cy = lane_sum(cy);
+  cz = lane_sum(cz);
+  if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, 1.0f);
 }
 
-// applyDeltaSolid, src/gpu/wgsl.js:361-366
+// Marks the fluid particles within contact range of solid i at position p
+// (GL lanes per solid). The bound is widened by 1e-5 so the set only grows:
+// the contacts pass makes the exact test.
+// Every lane of the warp calls it (the hash is shared by shuffles); only
+// active solids walk.
+__device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, float4 p,
+                                                bool act, int lane) {
+  CellHash ch;
+  group_cell_hash(p.x, p.y, p.z, P->inv_cell, ch);
+  if (!act) return;
+  const float rsum = P->solid_radius + P->fluid_radius;
+  const float lim2 = rsum * rsum * 1.00001f;
+  const float4* __restrict__ spos = v.spos;
+  uint32_t* __restrict__ mark = v.mark;
+  lane_slots<0>(v, ch, lane, [&](uint32_t e) {
+    const float4 pj = spos[e];
+    const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+    if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
+  });
+}
+
+// applyDeltaSolid, src/gpu/wgsl.js:361-366. With MARK (last iteration of the
+// solve) GL lanes per solid also mark the fluid near its final position for
+// the contacts pass; the fluid positions are final by then.
+template <bool MARK>
 __global__ void __launch_bounds__(256) k_apply_solid(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.S) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
+  const int t = UPBD_TID;
+  const int i = MARK ? t / GL : t;
+  const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
+  if (!MARK && !act) return;
   const float w = P->omega;
-  float4 p = v.pos[i];
-  const float4 d = v.delta[i];
-  p.x = p.x + d.x * w; p.y = p.y + d.y * w; p.z = p.z + d.z * w;
-  v.pos[i] = p;
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (act) {
+    p = v.pos[i];
+    const float4 d = v.delta[i];
+    p.x = p.x + d.x * w; p.y = p.y + d.y * w; p.z = p.z + d.z * w;
+  }
+  if (!MARK) {
+    v.pos[i] = p;
+    v.spos[v.slot[i]] = p;
+    return;
+  }
+  const int lane = threadIdx.x & (GL - 1);
+  if (act && lane == 0) {
+    v.pos[i] = p;
+    v.spos[v.slot[i]] = p;
+  }
+  if (P->use_mark) mark_fluid_near(v, P, p, act, lane);
+}
+
+// Contact marking on its own (when the solve's last position update is not
+// applyDeltaSolid, or there are no solve iterations).
+__global__ void __launch_bounds__(256) k_contact_mark(SimView v, const DevParams* __restrict__ P) {
+  if (!P->use_mark) return;
+  const int t = UPBD_TID;
+  const int i = t / GL;
+  const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
+  mark_fluid_near(v, P, act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (GL - 1));
 }
 
 // latticeRest, src/gpu/wgsl.js:373-381
@@ -458,6 +562,7 @@ __global__ void __launch_bounds__(256) k_apply_solid_contacts(SimView v, const D
   float4 p = v.pos[i];
   p.x = p.x + dx; p.y = p.y + dy; p.z = p.z + dz;
   v.pos[i] = p;
+  v.spos[v.slot[i]] = p;
 }
 
 __device__ __forceinline__ void cross3(float ax, float ay, float az, float bx, float by, float bz,
@@ -570,53 +675,64 @@ __device__ __forceinline__ void tet_update(const SimView& v, const DevParams* __
     }
 }
 
-__device__ __forceinline__ void contacts_one(const SimView& v, const DevParams* __restrict__ P, int i) {
-  if (!(v.flags[i] & F_ACTIVE)) return;
+// contacts for particle i, lane `lane` of its GL; every lane reaches the
+// shuffles. Fluid particles that no solid marked have no contact and skip the
+// walk (their correction is zero either way).
+__device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams* __restrict__ P, int i, int lane,
+                                              int nc) {
+  const bool act = i < nc && (v.flags[i] & F_ACTIVE);
   const bool iSolid = i < v.S;
-  const float4 pi = v.pos[i];
-  const float wi = pi.w;
-  const float rs = P->solid_radius, rf = P->fluid_radius, scale = P->contact_scale;
-  const float ri = iSolid ? rs : rf;
-  const uint32_t mask = (uint32_t)v.T - 1u;
-  CellHash ch;
-  ch.init(pi.x, pi.y, pi.z, P->inv_cell);
+  const bool walk = act && (iSolid || !P->use_mark || v.mark[i] != 0u);
   float cx = 0.f, cy = 0.f, cz = 0.f, cnt = 0.f;
-  for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++)
-      for (int c = 0; c < 3; c++) {
-        const uint32_t hb = ch.bucket(a, b, c, mask);
-        const uint32_t e1 = v.start[hb + 1];
-        for (uint32_t e = v.start[hb]; e < e1; e++) {
-          const uint32_t j = v.entries[e];
-          if (j == (uint32_t)i) continue;
-          const bool jSolid = j < (uint32_t)v.S;
-          if (iSolid == jSolid) continue;
-          const float4 pj = v.pos[j];
-          const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-          const float rsum = ri + (jSolid ? rs : rf);
-          const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-          if (d2 >= rsum * rsum || d2 < 1e-12f) continue;
-          const float wsum = wi + pj.w;
-          if (wsum == 0.f) continue;
-          const float d = sqrtf(d2);
-          const float f = (rsum - d) / d * wi / wsum * scale;
-          cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
-          cnt = cnt + 1.0f;
-        }
-      }
-  v.delta[i] = make_float4(cx, cy, cz, cnt);
+  const float4 pi = walk ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  CellHash ch;
+  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
+  if (walk) {
+    const float wi = pi.w;
+    const float rs = P->solid_radius, rf = P->fluid_radius, scale = P->contact_scale;
+    // a solid meets the fluid part of each bucket, a fluid particle the solid
+    // part (fluid-fluid is DDR's job, solid-solid the contact cache's)
+    const float ri = iSolid ? rs : rf;
+    const float rsum = ri + (iSolid ? rf : rs);
+    const float4* __restrict__ spos = v.spos;
+    auto pair = [&](uint32_t e) {
+      const float4 pj = spos[e];
+      const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
+      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      if (d2 >= rsum * rsum || d2 < 1e-12f) return;
+      const float wsum = wi + pj.w;
+      if (wsum == 0.f) return;
+      const float d = sqrtf(d2);
+      const float f = (rsum - d) / d * wi / wsum * scale;
+      cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
+      cnt = cnt + 1.0f;
+    };
+    if (iSolid)
+      lane_slots<0>(v, ch, lane, pair);
+    else
+      lane_slots<1>(v, ch, lane, pair);
+  }
+  cx = lane_sum(cx);
+  cy = lane_sum(cy);
+  cz = lane_sum(cz);
+  cnt = lane_sum(cnt);
+  if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, cnt);
 }
 
+// nb_pad is nb + nt rounded up to a multiple of 32, so the contact threads
+// start on a warp boundary and whole warps reach lane_sum's shuffles.
 __global__ void __launch_bounds__(256) k_bond_contacts(SimView v, const DevParams* __restrict__ P,
-                                                       int nb, int nt, int nc) {
+                                                       int nb, int nt, int nb_pad, int nc) {
   const int t = UPBD_TID;
-  if (t < nb) {
-    bond_update(v, P, t);
-  } else if (t < nb + nt) {
-    tet_update(v, P, t - nb);
-  } else if (t < nb + nt + nc) {
-    contacts_one(v, P, t - nb - nt);
+  if (t < nb_pad) {
+    if (t < nb)
+      bond_update(v, P, t);
+    else if (t < nb + nt)
+      tet_update(v, P, t - nb);
+    return;
   }
+  const int c = t - nb_pad;
+  contacts_lane(v, P, c / GL, c & (GL - 1), nc);
 }
 
 // -------------------------------- apply + bounds + velocity (per particle)
@@ -644,8 +760,10 @@ __global__ void __launch_bounds__(256) k_apply_bounds_vel(SimView v, const DevPa
     }
     p.x = p.x + dx; p.y = p.y + dy; p.z = p.z + dz;
   }
+  const uint32_t sl = v.slot[i];
   if (stage < 2) {
     v.pos[i] = p;
+    v.spos[sl] = p;
     return;
   }
   // bounds
@@ -679,7 +797,14 @@ __global__ void __launch_bounds__(256) k_apply_bounds_vel(SimView v, const DevPa
   }
   p.x = px; p.y = py; p.z = pz;
   v.pos[i] = p;
-  if (stage < 3 || culled) return;
+  v.spos[sl] = p;
+  if (stage < 3) return;
+  if (culled) {
+    // xsph still reads a culled neighbour's velocity (src/gpu/wgsl.js:761
+    // does not test its flag): its slot keeps the unchanged velocity
+    v.svel[sl] = v.vel[i];
+    return;
+  }
   // velocityUpdate
   const float h = P->h;
   float vx = (p.x - pv.x) / h, vy = (p.y - pv.y) / h, vz = (p.z - pv.z) / h;
@@ -694,7 +819,9 @@ __global__ void __launch_bounds__(256) k_apply_bounds_vel(SimView v, const DevPa
   }
   if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) atomicOr(&v.scratch[SCR_HEALTH], 1u);
   const float vw = v.vel[i].w;
-  v.vel[i] = make_float4(vx, vy, vz, vw);
+  const float4 nv = make_float4(vx, vy, vz, vw);
+  v.vel[i] = nv;
+  v.svel[sl] = nv;
 }
 
 // solidVisc, src/gpu/wgsl.js:717-735
@@ -735,40 +862,44 @@ __global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) {
 
 // xsph, src/gpu/wgsl.js:745-771
 __global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) {
-  const int i = v.S + (int)UPBD_TID;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 pi = v.pos[i];
-  const float H = P->fluid_h, H2 = H * H;
-  const uint32_t mask = (uint32_t)v.T - 1u;
-  CellHash ch;
-  ch.init(pi.x, pi.y, pi.z, P->inv_cell);
+  const int t = UPBD_TID;
+  const int lane = threadIdx.x & (GL - 1);
+  const int i = v.S + t / GL;
+  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
   float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
-  for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++)
-      for (int c = 0; c < 3; c++) {
-        const uint32_t hb = ch.bucket(a, b, c, mask);
-        const uint32_t e1 = v.start[hb + 1];
-        for (uint32_t e = v.start[hb]; e < e1; e++) {
-          const uint32_t j = v.entries[e];
-          if (j == (uint32_t)i || j < (uint32_t)v.S) continue;
-          const float4 pj = v.pos[j];
-          const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-          if (dot3(ex, ey, ez, ex, ey, ez) >= H2) continue;
-          const float4 vj = v.vel[j];
-          sx = sx + vj.x; sy = sy + vj.y; sz = sz + vj.z;
-          m = m + 1.0f;
-        }
-      }
-  const float4 vi = v.vel[i];
-  float vx = vi.x, vy = vi.y, vz = vi.z;
-  if (m > 0.f) {
-    const float mu = P->viscosity;
-    vx = vx + mu * (sx / m - vx);
-    vy = vy + mu * (sy / m - vy);
-    vz = vz + mu * (sz / m - vz);
+  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  CellHash ch;
+  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
+  if (act) {
+    const float H = P->fluid_h, H2 = H * H;
+    const float4* __restrict__ spos = v.spos;
+    const float4* __restrict__ svel = v.svel;
+    const uint32_t myslot = v.slot[i];
+    lane_slots<0>(v, ch, lane, [&](uint32_t e) {
+      const float4 pj = spos[e];
+      if (e == myslot) return;
+      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+      if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
+      const float4 vj = svel[e];
+      sx = sx + vj.x; sy = sy + vj.y; sz = sz + vj.z;
+      m = m + 1.0f;
+    });
   }
-  v.delta[i] = make_float4(vx, vy, vz, m);
+  sx = lane_sum(sx);
+  sy = lane_sum(sy);
+  sz = lane_sum(sz);
+  m = lane_sum(m);
+  if (act && lane == 0) {
+    const float4 vi = v.vel[i];
+    float vx = vi.x, vy = vi.y, vz = vi.z;
+    if (m > 0.f) {
+      const float mu = P->viscosity;
+      vx = vx + mu * (sx / m - vx);
+      vy = vy + mu * (sy / m - vy);
+      vz = vz + mu * (sz / m - vz);
+    }
+    v.delta[i] = make_float4(vx, vy, vz, m);
+  }
 }
 
 // xsphApply, src/gpu/wgsl.js:773-778

@@ -28,6 +28,25 @@ template <class R> static inline R signR(R x) { return x > 0 ? R(1) : (x < 0 ? R
 static constexpr uint32_t F_ACTIVE = 1u, F_GRABBED = 2u;
 static constexpr uint32_t C_K = 40u;  // src/gpu/wgsl.js:25
 
+// Summation order of the neighbour gathers (fluidDensity, fluidDisp, xsph,
+// contacts). The reference sums one particle's neighbours in any order its
+// invocation takes; this restatement fixes the order the CUDA kernels use, so
+// the two agree bit for bit: the 27 neighbour cells k = (dx+1)*9 + (dy+1)*3 +
+// (dz+1) are dealt to GL = 8 lanes (lane l walks k = l, l+8, l+16, l+24, each
+// bucket's entries in order), every lane sums from zero, and the eight
+// partials combine as ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
+static constexpr int GL = 8;
+template <class R> static inline R lane_reduce(const R* p) {
+  return ((p[0] + p[4]) + (p[2] + p[6])) + ((p[1] + p[5]) + (p[3] + p[7]));
+}
+template <class Sim, class V, class Fn> static inline void lane_walk(const Sim& s, const V& pi, Fn&& fn) {
+  for (int l = 0; l < GL; l++)
+    for (int k = l; k < 27; k += GL) {
+      const uint32_t h = s.cellHashOf(pi, k / 9 - 1, (k / 3) % 3 - 1, k % 3 - 1);
+      for (uint32_t e = s.start[h]; e < s.start[h + 1]; e++) fn(l, s.entries[e]);
+    }
+}
+
 template <class R> int O2Sim<R>::create(const upbd_scene_desc& d, const upbd_params& p) {
   desc = d;
   if (d.solid_dim < 0 || d.solid_dim2 < 0 || d.max_fluid < 0) return UPBD_ERR_INVALID;
@@ -325,23 +344,17 @@ template <class R> void O2Sim<R>::passDensity() {
   for (int i = S; i < N; i++) {
     if (!(flags[i] & F_ACTIVE)) continue;
     const V4<R> pi = pos[i];
-    R rho = 0, rhoNear = 0;
-    for (int dx = -1; dx <= 1; dx++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dz = -1; dz <= 1; dz++) {
-          const uint32_t h = cellHashOf(pi, dx, dy, dz);
-          for (uint32_t e = start[h]; e < start[h + 1]; e++) {
-            const uint32_t j = entries[e];
-            if (j == (uint32_t)i || j < (uint32_t)S) continue;
-            const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
-            const R d2 = dot3(ex, ey, ez, ex, ey, ez);
-            if (d2 >= H2) continue;
-            const R q = LIT(1.0) - std::sqrt(d2) / H;
-            rho = rho + q * q;
-            rhoNear = rhoNear + q * q * q;
-          }
-        }
-    density[i] = V2<R>{rho, rhoNear};
+    R rho[GL] = {}, rhoNear[GL] = {};
+    lane_walk(*this, pi, [&](int l, uint32_t j) {
+      if (j == (uint32_t)i || j < (uint32_t)S) return;
+      const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
+      const R d2 = dot3(ex, ey, ez, ex, ey, ez);
+      if (d2 >= H2) return;
+      const R q = LIT(1.0) - std::sqrt(d2) / H;
+      rho[l] = rho[l] + q * q;
+      rhoNear[l] = rhoNear[l] + q * q * q;
+    });
+    density[i] = V2<R>{lane_reduce(rho), lane_reduce(rhoNear)};
   }
 }
 
@@ -355,27 +368,22 @@ template <class R> void O2Sim<R>::passDisp() {
     const V4<R> pi = pos[i];
     const R Pi = P.stiffness * (density[i].x - P.restDensity);
     const R PNi = P.nearStiffness * density[i].y;
-    R sx = 0, sy = 0, sz = 0;
-    for (int dx = -1; dx <= 1; dx++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dz = -1; dz <= 1; dz++) {
-          const uint32_t h = cellHashOf(pi, dx, dy, dz);
-          for (uint32_t e = start[h]; e < start[h + 1]; e++) {
-            const uint32_t j = entries[e];
-            if (j == (uint32_t)i || j < (uint32_t)S) continue;
-            const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
-            const R d2 = dot3(ex, ey, ez, ex, ey, ez);
-            if (d2 >= H2 || d2 < LIT(1e-12)) continue;
-            const R d = std::sqrt(d2);
-            const R q = LIT(1.0) - d / H;
-            const R Pj = P.stiffness * (density[j].x - P.restDensity);
-            const R PNj = P.nearStiffness * density[j].y;
-            R D = LIT(0.25) * ((Pi + Pj) * q + (PNi + PNj) * q * q);
-            D = clampR(D, -maxPair, maxPair);
-            const R f = D / d;
-            sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
-          }
-        }
+    R px[GL] = {}, py[GL] = {}, pz[GL] = {};
+    lane_walk(*this, pi, [&](int l, uint32_t j) {
+      if (j == (uint32_t)i || j < (uint32_t)S) return;
+      const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
+      const R d2 = dot3(ex, ey, ez, ex, ey, ez);
+      if (d2 >= H2 || d2 < LIT(1e-12)) return;
+      const R d = std::sqrt(d2);
+      const R q = LIT(1.0) - d / H;
+      const R Pj = P.stiffness * (density[j].x - P.restDensity);
+      const R PNj = P.nearStiffness * density[j].y;
+      R D = LIT(0.25) * ((Pi + Pj) * q + (PNi + PNj) * q * q);
+      D = clampR(D, -maxPair, maxPair);
+      const R f = D / d;
+      px[l] = px[l] - ex * f; py[l] = py[l] - ey * f; pz[l] = pz[l] - ez * f;
+    });
+    R sx = lane_reduce(px), sy = lane_reduce(py), sz = lane_reduce(pz);
     const R s2 = dot3(sx, sy, sz, sx, sy, sz);
     if (s2 > maxTotal * maxTotal) {
       const R f = maxTotal / std::sqrt(s2);
@@ -467,10 +475,13 @@ template <class R> void O2Sim<R>::passSolidSolve() {
     if (!(flags[i] & F_ACTIVE)) continue;
     const V4<R> pi = pos[i];
     const R wi = pi.w;
-    R cx = 0, cy = 0, cz = 0;
+    // incident constraint k of the CSR goes to lane (k - st) % GL; lanes
+    // combine like the neighbour gathers (see lane_reduce)
+    R cx[GL] = {}, cy[GL] = {}, cz[GL] = {};
     const uint32_t st = adj[i], en = adj[i + 1];
     const uint32_t degI = en - st;
     for (uint32_t k = st; k < en; k++) {
+      const int l = (int)((k - st) % GL);
       const uint32_t ci = adj[S + 1 + k];
       if (consAlive[ci] == 0) continue;
       const uint32_t other = (consA[ci] == (uint32_t)i) ? consB[ci] : consA[ci];
@@ -485,9 +496,9 @@ template <class R> void O2Sim<R>::passSolidSolve() {
       const R s = LIT(1.0) / (R)std::max(degI, degJ);
       const R dl = -(d - rest) / (wsum + alpha);
       const R f = dl * wi / d * s;
-      cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
+      cx[l] = cx[l] + ex * f; cy[l] = cy[l] + ey * f; cz[l] = cz[l] + ez * f;
     }
-    delta[i] = V4<R>{cx, cy, cz, LIT(1.0)};
+    delta[i] = V4<R>{lane_reduce(cx), lane_reduce(cy), lane_reduce(cz), LIT(1.0)};
   }
 }
 
@@ -657,31 +668,25 @@ template <class R> void O2Sim<R>::passContacts() {
     const V4<R> pi = pos[i];
     const R wi = pi.w;
     const R ri = iSolid ? P.solidRadius : P.fluidRadius;
-    R cx = 0, cy = 0, cz = 0, cnt = 0;
-    for (int dx = -1; dx <= 1; dx++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dz = -1; dz <= 1; dz++) {
-          const uint32_t h = cellHashOf(pi, dx, dy, dz);
-          for (uint32_t e = start[h]; e < start[h + 1]; e++) {
-            const uint32_t j = entries[e];
-            if (j == (uint32_t)i) continue;
-            const bool jSolid = j < (uint32_t)S;
-            if (iSolid == jSolid) continue;
-            const R ex = pi.x - pos[j].x, ey = pi.y - pos[j].y, ez = pi.z - pos[j].z;
-            const R rj = jSolid ? P.solidRadius : P.fluidRadius;
-            const R rsum = ri + rj;
-            const R d2 = dot3(ex, ey, ez, ex, ey, ez);
-            if (d2 >= rsum * rsum || d2 < LIT(1e-12)) continue;
-            const R wj = pos[j].w;
-            const R wsum = wi + wj;
-            if (wsum == 0) continue;
-            const R d = std::sqrt(d2);
-            const R f = (rsum - d) / d * wi / wsum * P.contactScale;
-            cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
-            cnt = cnt + LIT(1.0);
-          }
-        }
-    delta[i] = V4<R>{cx, cy, cz, cnt};
+    R cx[GL] = {}, cy[GL] = {}, cz[GL] = {}, cnt[GL] = {};
+    lane_walk(*this, pi, [&](int l, uint32_t j) {
+      if (j == (uint32_t)i) return;
+      const bool jSolid = j < (uint32_t)S;
+      if (iSolid == jSolid) return;
+      const R ex = pi.x - pos[j].x, ey = pi.y - pos[j].y, ez = pi.z - pos[j].z;
+      const R rj = jSolid ? P.solidRadius : P.fluidRadius;
+      const R rsum = ri + rj;
+      const R d2 = dot3(ex, ey, ez, ex, ey, ez);
+      if (d2 >= rsum * rsum || d2 < LIT(1e-12)) return;
+      const R wj = pos[j].w;
+      const R wsum = wi + wj;
+      if (wsum == 0) return;
+      const R d = std::sqrt(d2);
+      const R f = (rsum - d) / d * wi / wsum * P.contactScale;
+      cx[l] = cx[l] + ex * f; cy[l] = cy[l] + ey * f; cz[l] = cz[l] + ez * f;
+      cnt[l] = cnt[l] + LIT(1.0);
+    });
+    delta[i] = V4<R>{lane_reduce(cx), lane_reduce(cy), lane_reduce(cz), lane_reduce(cnt)};
   }
 }
 
@@ -788,20 +793,15 @@ template <class R> void O2Sim<R>::passXsph() {
   for (int i = S; i < N; i++) {
     if (!(flags[i] & F_ACTIVE)) continue;
     const V4<R> pi = pos[i];
-    R sx = 0, sy = 0, sz = 0, m = 0;
-    for (int dx = -1; dx <= 1; dx++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dz = -1; dz <= 1; dz++) {
-          const uint32_t h = cellHashOf(pi, dx, dy, dz);
-          for (uint32_t e = start[h]; e < start[h + 1]; e++) {
-            const uint32_t j = entries[e];
-            if (j == (uint32_t)i || j < (uint32_t)S) continue;
-            const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
-            if (dot3(ex, ey, ez, ex, ey, ez) >= H2) continue;
-            sx = sx + vel[j].x; sy = sy + vel[j].y; sz = sz + vel[j].z;
-            m = m + LIT(1.0);
-          }
-        }
+    R qx[GL] = {}, qy[GL] = {}, qz[GL] = {}, qm[GL] = {};
+    lane_walk(*this, pi, [&](int l, uint32_t j) {
+      if (j == (uint32_t)i || j < (uint32_t)S) return;
+      const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
+      if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
+      qx[l] = qx[l] + vel[j].x; qy[l] = qy[l] + vel[j].y; qz[l] = qz[l] + vel[j].z;
+      qm[l] = qm[l] + LIT(1.0);
+    });
+    const R sx = lane_reduce(qx), sy = lane_reduce(qy), sz = lane_reduce(qz), m = lane_reduce(qm);
     R vx = vel[i].x, vy = vel[i].y, vz = vel[i].z;
     if (m > 0) {
       vx = vx + P.viscosity * (sx / m - vx);
