@@ -115,6 +115,7 @@ _SIGS = [
     ("upbd_read_tets", C.c_int, [_P, _U]),
     ("upbd_groups", C.c_int, [_P, C.POINTER(C.c_int32)]),
     ("upbd_grid_build", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
+    ("upbd_grid_build_noalloc", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
     ("upbd_launch_count", C.c_uint64, [_P]),
     ("upbd_profile_frame", C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(C.c_double), _U]),
     ("upbd_kernel_name", C.c_char_p, [C.c_int32]),

@@ -1388,3 +1388,104 @@ int upbd_profile_frame(upbd_sim* s, double dt, int32_t substeps, double* ms, uin
 }
 
 }  // extern "C"
+
+// ===================================================== allocation-free grid build
+// upbd_grid_build takes its scratch (bucket counts, arrival tickets, bucket of
+// each particle, the unordered scatter, scan tile totals) from a pool that it
+// grows with cudaMalloc. Some callers cannot allocate device memory at all: a
+// host that embeds this library in a runtime which owns the device-memory
+// budget and refuses allocations it did not make, or a frame loop that must
+// never stall on an allocation. For them, upbd_grid_build_noalloc keeps the
+// same scratch in this file-scope array, which lives in the library image:
+// every GPU that loads the library holds its 4 MiB until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxN = 1 << 18;  // particles per call
+constexpr int kNoAllocMaxT = 1 << 18;  // hash buckets per call
+constexpr size_t kNoAllocTiles = (kNoAllocMaxT + SCAN_TILE - 1) / SCAN_TILE;
+// word offsets inside the array
+constexpr size_t kNaCounts = 0;
+constexpr size_t kNaTicket = kNaCounts + kNoAllocMaxT;
+constexpr size_t kNaCell = kNaTicket + kNoAllocMaxN;
+constexpr size_t kNaTmp = kNaCell + kNoAllocMaxN;
+constexpr size_t kNaTiles = kNaTmp + kNoAllocMaxN;
+constexpr size_t kNaParams = ((kNaTiles + kNoAllocTiles + 63) / 64) * 64;  // 256-byte aligned
+constexpr size_t kNaWords = kNaParams + (sizeof(DevParams) + 3) / 4;
+
+__device__ __align__(256) uint32_t g_grid_scratch[kNaWords];
+
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_ptr[64] = {};  // device address of g_grid_scratch, per device
+
+// The hash reads 1/cell_size from a params block: set it on the device from
+// a kernel argument (no host-to-device copy, no staging buffer).
+__global__ void k_noalloc_params(DevParams* p, double inv_cell) { p->inv_cell = inv_cell; }
+
+// counts[h] = offsets[h+1] - offsets[h] (the scan clears its own counts)
+__global__ void k_counts_from_offsets(const uint32_t* __restrict__ offsets, uint32_t* __restrict__ counts, int T) {
+  const int h = UPBD_TID;
+  if (h < T) counts[h] = offsets[h + 1] - offsets[h];
+}
+
+}  // namespace
+
+extern "C" int upbd_grid_build_noalloc(const void* pos4, const void* flags, int32_t n, int32_t table_size,
+                                       double cell_size, void* counts, void* offsets, void* entries,
+                                       void* stream) {
+  if (n < 0 || (n > 0 && (!pos4 || !flags || !entries)) || !offsets)
+    return fail(nullptr, UPBD_ERR_INVALID, "bad grid_build_noalloc arguments");
+  if (table_size < 1 || (table_size & (table_size - 1)))
+    return fail(nullptr, UPBD_ERR_INVALID, "table_size must be a power of two");
+  if (n > kNoAllocMaxN || table_size > kNoAllocMaxT)
+    return fail(nullptr, UPBD_ERR_CAPACITY,
+                "grid_build_noalloc handles at most 262144 particles and 262144 buckets per call "
+                "(its scratch is a fixed array in the library)");
+  if (!(cell_size > 0)) return fail(nullptr, UPBD_ERR_INVALID, "cell_size must be > 0");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return fail(nullptr, UPBD_ERR_NO_DEVICE, "no current CUDA device");
+  uint32_t* w = nullptr;
+  {
+    // set-up, once per device and with that device current: the array's name
+    // is a host-side stand-in, the kernels need its device address
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_grid_scratch);
+      if (e != cudaSuccess)
+        return fail(nullptr, UPBD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = (uint32_t*)p;
+    }
+    w = g_noalloc_ptr[dev];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int tiles = (table_size + SCAN_TILE - 1) / SCAN_TILE;
+  SimView v{};
+  v.pos = (float4*)pos4;
+  v.flags = (uint32_t*)flags;
+  v.N = n;
+  v.T = table_size;
+  v.num_tiles = tiles;
+  v.counts = w + kNaCounts;
+  v.ticket = w + kNaTicket;
+  v.cell = w + kNaCell;
+  v.tmp = w + kNaTmp;
+  v.tile_sum = w + kNaTiles;
+  v.start = (uint32_t*)offsets;
+  v.entries = (uint32_t*)entries;
+  DevParams* dp = (DevParams*)(w + kNaParams);
+  // the array keeps the previous call's contents: counts and tile totals
+  // must start at zero
+  cudaError_t e = cudaMemsetAsync(v.counts, 0, (size_t)table_size * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(v.tile_sum, 0, (size_t)tiles * 4, st);
+  if (e != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, std::string("scratch clear: ") + cudaGetErrorString(e));
+  k_noalloc_params<<<1, 1, 0, st>>>(dp, 1.0 / cell_size);
+  k_integrate_count<false, true><<<blocks_for(n), 256, 0, st>>>(v, dp);
+  k_scan<<<tiles, SCAN_THREADS, 0, st>>>(v);
+  k_scatter<<<blocks_for(std::max(n, tiles)), 256, 0, st>>>(v);
+  k_rankfix<<<blocks_for(n), 256, 0, st>>>(v);
+  if (counts) k_counts_from_offsets<<<blocks_for(table_size), 256, 0, st>>>(v.start, (uint32_t*)counts, table_size);
+  e = cudaPeekAtLastError();
+  if (e != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, cudaGetErrorString(e));
+  return UPBD_OK;
+}

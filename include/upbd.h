@@ -318,6 +318,26 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
                     double cell_size, void* counts, void* offsets, void* entries,
                     void* stream);
 
+/* The same hash-grid build for callers that cannot allocate device memory
+ * (this entry point has no counterpart in the reference). A host that embeds
+ * the library in a runtime owning the device-memory budget, which refuses
+ * allocations it did not make, or a frame loop that must not stall on an
+ * allocation, cannot use upbd_grid_build's cudaMalloc-grown scratch pool.
+ * This variant calls no cudaMalloc/cudaFree: its scratch is a fixed 4 MiB
+ * array inside the library, held by every GPU that loads the library until
+ * the process exits. Limits: n <= 262144 particles and table_size <= 262144
+ * buckets per call; larger sizes return UPBD_ERR_CAPACITY. Arguments and
+ * outputs are those of upbd_grid_build (counts may be NULL).
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture. Every call shares the one array: calls whose
+ * work overlaps on the GPU (other streams, other threads) race and corrupt
+ * each other's results, so order them on one stream or with events. Each call
+ * clears the parts of the array that must start at zero. */
+int upbd_grid_build_noalloc(const void* pos4, const void* flags, int32_t n, int32_t table_size,
+                            double cell_size, void* counts, void* offsets, void* entries,
+                            void* stream);
+
 /* Kernels this handle has launched so far (each replay of a captured frame
  * counts its kernel nodes). Instrumentation for benchmarks. */
 uint64_t upbd_launch_count(upbd_sim* sim);
