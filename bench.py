@@ -218,6 +218,8 @@ def main() -> None:
     ap.add_argument("--impl", default="upbd", choices=["upbd", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--profile-frames", type=int, default=20)
+    ap.add_argument("--profile-after", type=int, default=30,
+                    help="frames stepped from the initial state before the per-kernel profile")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -341,7 +343,7 @@ def main() -> None:
 
     # ---- per-kernel device times of eager frames (dominant kernel roofline)
     reset()
-    for _ in range(30):  # into a settled, interacting state
+    for _ in range(args.profile_after):  # into an interacting state
         sim.step(sc.dt, sc.substeps)
     sim.sync()
     P = args.profile_frames
