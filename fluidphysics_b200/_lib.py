@@ -70,6 +70,26 @@ class DevicePtrs(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in ("pos", "prev", "vel", "density", "flags", "cons", "stream")]
 
 
+class BatchDesc(C.Structure):
+    """upbd_batch_desc (include/upbd_batch.h)."""
+    _fields_ = [
+        ("device", C.c_int32), ("solid_iters", C.c_int32), ("features", C.c_uint32),
+        ("max_scenes", C.c_int32), ("block_threads", C.c_int32), ("ctas_per_sm", C.c_int32),
+        ("hbm_budget", C.c_uint64), ("reserved", C.c_int32 * 8),
+    ]
+
+
+class BatchInfo(C.Structure):
+    """upbd_batch_info (include/upbd_batch.h)."""
+    _fields_ = [
+        ("scenes", C.c_int32), ("max_scenes", C.c_int32), ("particles", C.c_int64), ("solids", C.c_int64),
+        ("bytes_in_use", C.c_uint64), ("bytes_reserved", C.c_uint64), ("hbm_budget", C.c_uint64),
+        ("frames", C.c_uint64), ("launches", C.c_uint64), ("block_threads", C.c_int32),
+        ("ctas_per_sm", C.c_int32), ("num_sms", C.c_int32), ("reserved0", C.c_int32),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
 # (name, restype, argtypes)
 _P = C.c_void_p
 _D3 = C.POINTER(C.c_double)
@@ -119,6 +139,28 @@ _SIGS = [
     ("upbd_launch_count", C.c_uint64, [_P]),
     ("upbd_profile_frame", C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(C.c_double), _U]),
     ("upbd_kernel_name", C.c_char_p, [C.c_int32]),
+    # scene batch (include/upbd_batch.h)
+    ("upbd_batch_default_desc", C.c_int, [C.POINTER(BatchDesc)]),
+    ("upbd_batch_create", C.c_int, [C.POINTER(BatchDesc), C.POINTER(_P)]),
+    ("upbd_batch_destroy", C.c_int, [_P]),
+    ("upbd_batch_last_error", C.c_char_p, [_P]),
+    ("upbd_batch_get_info", C.c_int, [_P, C.POINTER(BatchInfo)]),
+    ("upbd_batch_scene_bytes", C.c_int, [C.POINTER(SceneDesc), C.POINTER(C.c_uint64)]),
+    ("upbd_batch_add_scene", C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(Params), C.c_int32, _F, _F,
+                                       C.c_double, C.POINTER(C.c_int32)]),
+    ("upbd_batch_remove_scene", C.c_int, [_P, C.c_int32]),
+    ("upbd_batch_set_params", C.c_int, [_P, C.c_int32, C.POINTER(Params)]),
+    ("upbd_batch_step", C.c_int, [_P, C.c_double, C.c_int32]),
+    ("upbd_batch_sync", C.c_int, [_P]),
+    ("upbd_batch_set_stream", C.c_int, [_P, _P]),
+    ("upbd_batch_set_tuning", C.c_int, [_P, C.c_int32, C.c_int32]),
+    ("upbd_batch_read_state", C.c_int, [_P, C.c_int32, _F, _F, _F, _F, _U]),
+    ("upbd_batch_write_state", C.c_int, [_P, C.c_int32, _F, _F, _F, _F, _U]),
+    ("upbd_batch_read_constraints", C.c_int, [_P, C.c_int32, _U]),
+    ("upbd_batch_write_constraints", C.c_int, [_P, C.c_int32, _U]),
+    ("upbd_batch_scene_info", C.c_int, [_P, C.c_int32, C.POINTER(Info)]),
+    ("upbd_batch_active_count", C.c_int, [_P, C.c_int32, _U]),
+    ("upbd_batch_profile_frame", C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(C.c_double), _U]),
 ]
 KERNEL_KINDS = 32
 
@@ -158,6 +200,12 @@ def load(variant: str = "product") -> C.CDLL:
 def check(lib: C.CDLL, handle, rc: int) -> None:
     if rc != UPBD_OK:
         msg = lib.upbd_last_error(handle)
+        raise UpbdError(rc, msg.decode() if msg else "")
+
+
+def check_batch(lib: C.CDLL, handle, rc: int) -> None:
+    if rc != UPBD_OK:
+        msg = lib.upbd_batch_last_error(handle)
         raise UpbdError(rc, msg.decode() if msg else "")
 
 

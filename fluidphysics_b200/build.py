@@ -23,9 +23,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
           "-I", str(INCLUDE), "-Xptxas", "-warn-spills"]
 
+SOURCES = ["upbd.cu", "upbd_scene.cu", "upbd_batch.cu"]
 TARGETS = {
-    "libupbd.so": ["upbd.cu"],
-    "libupbd_parity.so": ["upbd.cu"],
+    "libupbd.so": SOURCES,
+    "libupbd_parity.so": SOURCES,
 }
 
 

@@ -1,11 +1,8 @@
-// sm_100a kernels of the unified-particle substep. Each kernel restates one
-// or more WGSL passes of the reference (src/gpu/wgsl.js, cited per kernel)
-// and keeps their floating-point operand order; passes that only touch a
-// particle's own slot are fused into one launch. All kernels are FP32 SIMT
-// gathers over HBM-resident state: there is no dense contraction on this
-// path, so the tensor cores have no role here.
+// Single-scene sm_100a kernels of libupbd: the per-pass wrappers around the
+// pass bodies of upbd_passes.cuh, and the tool kernels (emit, wedge cut,
+// pick, grab, drain) that run on demand.
 #pragma once
-#include "upbd_device.cuh"
+#include "upbd_passes.cuh"
 
 namespace upbd {
 
@@ -55,861 +52,59 @@ __global__ void k_emit_particles(SimView v, const float* __restrict__ p3,
   v.flags[slot] = F_ACTIVE;
 }
 
-// --------------------------------------------------- integrate + grid count
-// integrate (src/gpu/wgsl.js:121-160) fused with gridCount
-// (src/gpu/wgsl.js:173-178). The count keeps each particle's arrival ticket
-// and bumps its scan tile's total, so the scan needs no second pass.
+// ------------------------------------------------- single-scene kernels
+// One launch per pass over one scene: tile vb = blockIdx.x.
 template <bool INTEGRATE, bool COUNT>
 __global__ void __launch_bounds__(256) k_integrate_count(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.N) return;
-  uint32_t f = v.flags[i];
-  if (!(f & F_ACTIVE)) return;
-  float4 p4 = v.pos[i];
-  if (INTEGRATE) {
-    const float h = P->h;
-    const float4 vv = v.vel[i];
-    const float vx = vv.x, vz = vv.z;
-    const float vy = vv.y + P->gravity * h;
-    const float px = p4.x, py = p4.y, pz = p4.z;
-    float nx = px + vx * h, ny = py + vy * h, nz = pz + vz * h;
-    const float4 pv = v.prev[i];
-    float tw = pv.w;
-    bool slipped = false;
-    if (f & F_GRABBED) {
-      const float4 gd = P->grab_delta;
-      const float2 dn = v.density[i];
-      float tx = pv.w, ty = vv.w, tz = dn.x;
-      tx = tx + gd.x; ty = ty + gd.y; tz = tz + gd.z;
-      const float ex = nx - tx, ey = ny - ty, ez = nz - tz;
-      if (sqrtf(dot3(ex, ey, ez, ex, ey, ez)) > 1.0f) {
-        f &= ~F_GRABBED;
-        v.flags[i] = f;
-        v.vel[i] = make_float4(vx, vy, vz, 0.f);
-        slipped = true;
-      } else {
-        const float k = P->grab_k * dn.y;
-        float cx = (tx - nx) * k, cy = (ty - ny) * k, cz = (tz - nz) * k;
-        const float cl = sqrtf(dot3(cx, cy, cz, cx, cy, cz));
-        const float maxC = 0.05f;
-        if (cl > maxC) {
-          const float g = maxC / cl;
-          cx = cx * g; cy = cy * g; cz = cz * g;
-        }
-        nx = nx + cx; ny = ny + cy; nz = nz + cz;
-        tw = tx;
-        v.vel[i] = make_float4(vx, vy, vz, ty);
-        v.density[i] = make_float2(tz, dn.y);
-      }
-    } else {
-      v.vel[i] = make_float4(vx, vy, vz, vv.w);
-    }
-    (void)slipped;
-    v.prev[i] = make_float4(px, py, pz, tw);
-    p4 = make_float4(nx, ny, nz, p4.w);
-    v.pos[i] = p4;
-    if (i >= v.S) v.mark[i] = 0u;  // contact marks of this substep start clear
-  }
-  if (COUNT) {
-    const uint32_t h = cell_of(p4.x, p4.y, p4.z, P->inv_cell, (uint32_t)v.T - 1u);
-    v.cell[i] = h;
-    v.ticket[i] = atomicAdd(&v.counts[h], 1u);
-    atomicAdd(&v.tile_sum[h / SCAN_TILE], 1u);
-  }
+  b_integrate_count<INTEGRATE, COUNT>(v, P, blockIdx.x);
 }
-
-// ------------------------------------------------------------ exclusive scan
-// scanBlocks/scanPartials/scanApply (src/gpu/wgsl.js:180-236) as one launch:
-// block b first sums the totals of tiles < b (kept by the count), then scans
-// its own 2048 counts, writes start[], and clears the counts it read.
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan(SimView v) {
-  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
-  __shared__ uint32_t s_base;
-  const int tid = threadIdx.x;
-  const int lane = tid & 31, wid = tid >> 5;
-  // base = sum of totals of earlier tiles
-  uint32_t acc = 0;
-  for (int t = tid; t < (int)blockIdx.x; t += SCAN_THREADS) acc += v.tile_sum[t];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if (lane == 0) s_warp[wid] = acc;
-  __syncthreads();
-  if (tid == 0) {
-    uint32_t b = 0;
-    for (int w = 0; w < SCAN_THREADS / 32; w++) b += s_warp[w];
-    s_base = b;
-  }
-  __syncthreads();
-  const uint32_t base = s_base;
-  // thread-local scan of 8 counts
-  const long long t0 = (long long)blockIdx.x * SCAN_TILE + (long long)tid * 8;
-  uint32_t c[8];
-  uint32_t sum = 0;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const long long idx = t0 + k;
-    c[k] = (idx < v.T) ? v.counts[idx] : 0u;
-    sum += c[k];
-  }
-  // block exclusive scan of thread sums
-  uint32_t x = sum;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  __syncthreads();
-  if (lane == 31) s_warp[wid] = x;
-  __syncthreads();
-  uint32_t wbase = 0;
-  for (int w = 0; w < wid; w++) wbase += s_warp[w];
-  uint32_t run = base + wbase + x - sum;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const long long idx = t0 + k;
-    if (idx < v.T) {
-      v.start[idx] = run;
-      if (v.fend) v.fend[idx] = run;  // empty buckets; rankfix sets occupied ones
-      v.counts[idx] = 0u;  // ready for the next count
-    }
-    run += c[k];
-  }
-  if (blockIdx.x == gridDim.x - 1 && tid == SCAN_THREADS - 1) v.start[v.T] = run;
-}
-
-// Scatter by ticket (gridScatter, src/gpu/wgsl.js:238-245, without its
-// second atomic), and clear the tile totals for the next count.
-__global__ void __launch_bounds__(256) k_scatter(SimView v) {
-  const int i = UPBD_TID;
-  if (i < v.num_tiles) v.tile_sum[i] = 0u;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const uint32_t h = v.cell[i];
-  v.tmp[v.start[h] + v.ticket[i]] = (uint32_t)i;
-}
-
-// Deterministic membership: particle i goes to start[h] + #{j in bucket : j > i},
-// i.e. descending index inside a bucket, the order Solver._buildGrid's
-// `--cellStart[h]` scatter leaves (src/solver.js:182-183).
-__global__ void __launch_bounds__(256) k_rankfix(SimView v) {
-  const int i = UPBD_TID;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const uint32_t h = v.cell[i];
-  const uint32_t s = v.start[h], e = v.start[h + 1];
-  uint32_t rank = 0, solids = 0;
-  for (uint32_t k = s; k < e; k++) {
-    const uint32_t j = v.tmp[k];
-    rank += (j > (uint32_t)i) ? 1u : 0u;
-    solids += (j < (uint32_t)v.S) ? 1u : 0u;
-  }
-  v.entries[s + rank] = (uint32_t)i;
-  if (v.spos) {  // the stateless grid build has no bucket-ordered copies
-    v.slot[i] = s + rank;
-    v.spos[s + rank] = v.pos[i];
-    v.fend[h] = e - solids;  // every member writes the same value
-  }
-}
-
-// ------------------------------------------------------------------ fluid
-// The neighbour gathers run GL lanes per particle (see lane_slots): a warp
-// holds 32/GL particles, every lane reaches the shuffles, and lane 0 writes.
-
-// fluidDensity, src/gpu/wgsl.js:254-279
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(SimView v) { b_scan(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_scatter(SimView v) { b_scatter(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_rankfix(SimView v) { b_rankfix(v, blockIdx.x); }
 __global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __restrict__ P) {
-  const int t = UPBD_TID;
-  const int lane = threadIdx.x & (GL - 1);
-  const int i = v.S + t / GL;
-  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
-  float rho = 0.f, rhoNear = 0.f;
-  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  CellHash ch;
-  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  uint32_t myslot = 0;
-  if (act) {
-    const float H = P->fluid_h, H2 = H * H;
-    const float4* __restrict__ spos = v.spos;
-    myslot = v.slot[i];
-    const uint32_t FG = (uint32_t)v.F * GL;
-    const uint32_t g = (uint32_t)(i - v.S) * GL + lane;
-    uint32_t* __restrict__ nbr = v.nbr + g;
-    uint32_t cnt = 0;
-    lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-      const float4 pj = spos[e];
-      if (e == myslot) return;
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      if (d2 >= H2) return;
-      const float q = 1.0f - sqrtf(d2) / H;
-      rho = rho + q * q;
-      rhoNear = rhoNear + q * q * q;
-      if (cnt < NL) nbr[cnt * FG] = e;  // for fluidDisp, same positions
-      cnt++;
-    });
-    v.ncount[g] = cnt;
-  }
-  rho = lane_sum(rho);
-  rhoNear = lane_sum(rhoNear);
-  if (act && lane == 0) {
-    const float2 d = make_float2(rho, rhoNear);
-    v.density[i] = d;
-    v.sdens[myslot] = d;
-  }
+  b_density(v, P, blockIdx.x);
 }
-
-// fluidDisp, src/gpu/wgsl.js:281-316
 __global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __restrict__ P) {
-  const int t = UPBD_TID;
-  const int lane = threadIdx.x & (GL - 1);
-  const int i = v.S + t / GL;
-  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
-  const float H = P->fluid_h, H2 = H * H;
-  float sx = 0.f, sy = 0.f, sz = 0.f;
-  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const uint32_t FG = (uint32_t)v.F * GL;
-  const uint32_t g = (uint32_t)(i - v.S) * GL + lane;
-  const uint32_t cnt = act ? v.ncount[g] : 0u;
-  CellHash ch;
-  if (__any_sync(0xffffffffu, cnt > NL)) group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  if (act) {
-    const float maxPair = 0.05f * H;
-    const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
-    const float2 di = v.density[i];
-    const float Pi = k * (di.x - rho0);
-    const float PNi = kn * di.y;
-    const float4* __restrict__ spos = v.spos;
-    const float2* __restrict__ sdens = v.sdens;
-    auto pair = [&](uint32_t e) {
-      const float4 pj = spos[e];
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      if (d2 >= H2 || d2 < 1e-12f) return;
-      const float d = sqrtf(d2);
-      const float q = 1.0f - d / H;
-      const float2 dj = sdens[e];
-      const float Pj = k * (dj.x - rho0);
-      const float PNj = kn * dj.y;
-      float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
-      D = clampf(D, -maxPair, maxPair);
-      const float f = D / d;
-      sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
-    };
-    // the density pass listed this lane's in-range neighbours at these same
-    // positions and in walk order; a lane whose list overflowed walks again
-    if (cnt <= NL) {
-      const uint32_t* __restrict__ nbr = v.nbr + g;
-      for (uint32_t c = 0; c < cnt; c++) pair(__ldg(&nbr[c * FG]));
-    } else {
-      const uint32_t myslot = v.slot[i];
-      lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-        if (e != myslot) pair(e);
-      });
-    }
-  }
-  sx = lane_sum(sx);
-  sy = lane_sum(sy);
-  sz = lane_sum(sz);
-  if (act && lane == 0) {
-    const float maxTotal = 0.35f * H;
-    const float s2 = dot3(sx, sy, sz, sx, sy, sz);
-    if (s2 > maxTotal * maxTotal) {
-      const float f = maxTotal / sqrtf(s2);
-      sx = sx * f; sy = sy * f; sz = sz * f;
-    }
-    v.delta[i] = make_float4(sx, sy, sz, 1.0f);
-  }
+  b_disp(v, P, blockIdx.x);
 }
-
-// applyDeltaFluid, src/gpu/wgsl.js:318-323 (standalone form)
-__global__ void k_apply_fluid(SimView v) {
-  const int i = v.S + (int)UPBD_TID;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  float4 p = v.pos[i];
-  const float4 d = v.delta[i];
-  p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
-  v.pos[i] = p;
-  v.spos[v.slot[i]] = p;
-}
-
-// ------------------------------------------------------------------ solids
-// solidSolve, src/gpu/wgsl.js:326-359, GL lanes per solid: lane l takes the
-// incident constraints k = st+l, st+l+GL, ... of the static CSR, whose other
-// endpoint and pair scale 1/max(deg_i, deg_j) are precomputed (both are fixed
-// for the life of the scene); the partials combine like lane_sum.
-// Threads from solid_pad on (a warp multiple, so the solve's warps are whole)
-// apply the fluid displacement when APPLY_FLUID (applyDeltaFluid,
-// src/gpu/wgsl.js:318-323): the solve reads solid positions only.
+__global__ void __launch_bounds__(256) k_apply_fluid(SimView v) { b_apply_fluid(v, blockIdx.x); }
 template <bool APPLY_FLUID>
 __global__ void __launch_bounds__(256) k_solid_solve(SimView v, const DevParams* __restrict__ P, int solid_pad) {
-  const int t = UPBD_TID;
-  if (t >= solid_pad) {
-    const int i = v.S + (t - solid_pad);
-    if (APPLY_FLUID && i < v.N && (v.flags[i] & F_ACTIVE)) {
-      float4 p = v.pos[i];
-      const float4 d = v.delta[i];
-      p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
-      v.pos[i] = p;
-      v.spos[v.slot[i]] = p;
-    }
-    return;
-  }
-  const int i = t / GL;
-  const int lane = threadIdx.x & (GL - 1);
-  const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
-  float cx = 0.f, cy = 0.f, cz = 0.f;
-  if (act) {
-    const float4 pi = v.pos[i];
-    const float wi = pi.w;
-    const float h = P->h;
-    const float alpha = P->compliance / (h * h);
-    const uint32_t st = v.adj[i], en = v.adj[i + 1];
-    const uint32_t* __restrict__ ids = v.adj + v.S + 1;
-    const uint4* __restrict__ cons = v.cons;
-    const float4* __restrict__ pos = v.pos;
-#pragma unroll 2
-    for (uint32_t k = st + lane; k < en; k += GL) {
-      const uint32_t ci = __ldg(&ids[k]);
-      const uint32_t other = __ldg(&v.adj_other[k]);
-      const float s = __ldg(&v.adj_scale[k]);
-      const float4 po = pos[other];
-      const uint2 rw = *reinterpret_cast<const uint2*>(&cons[ci].z);  // rest bits, alive
-      if (rw.y == 0u) continue;
-      const float rest = __uint_as_float(rw.x);
-      const float ex = pi.x - po.x, ey = pi.y - po.y, ez = pi.z - po.z;
-      const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
-      if (d < 1e-9f) continue;
-      const float wsum = wi + po.w;
-      if (wsum == 0.f) continue;
-      const float dl = -(d - rest) / (wsum + alpha);
-      const float f = dl * wi / d * s;
-      cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
-    }
-  }
-  cx = lane_sum(cx);
-  cy = lane_sum(cy);
-  cz = lane_sum(cz);
-  if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+  b_solid_solve<APPLY_FLUID>(v, P, solid_pad, blockIdx.x);
 }
-
-// Marks the fluid particles within contact range of solid i at position p
-// (GL lanes per solid). The bound is widened by 1e-5 so the set only grows:
-// the contacts pass makes the exact test.
-// Every lane of the warp calls it (the hash is shared by shuffles); only
-// active solids walk.
-__device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, float4 p,
-                                                bool act, int lane) {
-  CellHash ch;
-  group_cell_hash(p.x, p.y, p.z, P->inv_cell, ch);
-  if (!act) return;
-  const float rsum = P->solid_radius + P->fluid_radius;
-  const float lim2 = rsum * rsum * 1.00001f;
-  const float4* __restrict__ spos = v.spos;
-  uint32_t* __restrict__ mark = v.mark;
-  lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-    const float4 pj = spos[e];
-    const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-    if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
-  });
-}
-
-// applyDeltaSolid, src/gpu/wgsl.js:361-366. With MARK (last iteration of the
-// solve) GL lanes per solid also mark the fluid near its final position for
-// the contacts pass; the fluid positions are final by then.
 template <bool MARK>
 __global__ void __launch_bounds__(256) k_apply_solid(SimView v, const DevParams* __restrict__ P) {
-  const int t = UPBD_TID;
-  const int i = MARK ? t / GL : t;
-  const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
-  if (!MARK && !act) return;
-  const float w = P->omega;
-  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (act) {
-    p = v.pos[i];
-    const float4 d = v.delta[i];
-    p.x = p.x + d.x * w; p.y = p.y + d.y * w; p.z = p.z + d.z * w;
-  }
-  if (!MARK) {
-    v.pos[i] = p;
-    v.spos[v.slot[i]] = p;
-    return;
-  }
-  const int lane = threadIdx.x & (GL - 1);
-  if (act && lane == 0) {
-    v.pos[i] = p;
-    v.spos[v.slot[i]] = p;
-  }
-  if (P->use_mark) mark_fluid_near(v, P, p, act, lane);
+  b_apply_solid<MARK>(v, P, blockIdx.x);
 }
-
-// Contact marking on its own (when the solve's last position update is not
-// applyDeltaSolid, or there are no solve iterations).
 __global__ void __launch_bounds__(256) k_contact_mark(SimView v, const DevParams* __restrict__ P) {
-  if (!P->use_mark) return;
-  const int t = UPBD_TID;
-  const int i = t / GL;
-  const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
-  mark_fluid_near(v, P, act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (GL - 1));
+  b_contact_mark(v, P, blockIdx.x);
 }
-
-// latticeRest, src/gpu/wgsl.js:373-381
-__device__ __forceinline__ float lattice_rest(const SimView& v, float spacing, uint32_t a0, uint32_t b0) {
-  uint32_t a = a0, b = b0, D = (uint32_t)v.dim1;
-  if (a0 >= (uint32_t)v.N1) { a = a0 - v.N1; b = b0 - v.N1; D = (uint32_t)(v.dim2 > 1 ? v.dim2 : 1); }
-  const float ax = (float)(a / (D * D)), ay = (float)((a / D) % D), az = (float)(a % D);
-  const float bx = (float)(b / (D * D)), by = (float)((b / D) % D), bz = (float)(b % D);
-  const float dx = ax - bx, dy = ay - by, dz = az - bz;
-  return spacing * sqrtf(dx * dx + dy * dy + dz * dz);
-}
-
-// latticeAdjacent, src/gpu/wgsl.js:409-416
-__device__ __forceinline__ bool lattice_adjacent(const SimView& v, uint32_t i, uint32_t j) {
-  if ((i >= (uint32_t)v.N1) != (j >= (uint32_t)v.N1)) return false;
-  uint32_t a = i, b = j, D = (uint32_t)v.dim1;
-  if (i >= (uint32_t)v.N1) { a = i - v.N1; b = j - v.N1; D = (uint32_t)(v.dim2 > 1 ? v.dim2 : 1); }
-  const int ax = (int)(a / (D * D)), ay = (int)((a / D) % D), az = (int)(a % D);
-  const int bx = (int)(b / (D * D)), by = (int)((b / D) % D), bz = (int)(b % D);
-  return abs(ax - bx) <= 1 && abs(ay - by) <= 1 && abs(az - bz) <= 1;
-}
-
-// isBonded, src/gpu/wgsl.js:599-607
-__device__ __forceinline__ bool is_bonded(const SimView& v, uint32_t i, uint32_t j) {
-  const uint32_t* ids = v.adj + v.S + 1;
-  for (uint32_t k = v.adj[i]; k < v.adj[i + 1]; k++) {
-    const uint4 c = v.cons[ids[k]];
-    if (c.w != 0u && (c.x == j || c.y == j)) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ float solid_rsum(const SimView& v, const DevParams* __restrict__ P,
-                                            uint32_t i, uint32_t j) {
-  const float rsum = 2.0f * P->solid_radius;
-  if (lattice_adjacent(v, i, j)) return mn(rsum, P->spacing * 0.97f);
-  return rsum;
-}
-
-// collectContacts, src/gpu/wgsl.js:532-560
 __global__ void __launch_bounds__(256) k_collect_contacts(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.S) return;
-  uint32_t cnt = 0;
-  if (v.flags[i] & F_ACTIVE) {
-    const float4 pi = v.pos[i];
-    const float margin = 2.0f * P->solid_radius;
-    const uint32_t mask = (uint32_t)v.T - 1u;
-    CellHash ch;
-    ch.init(pi.x, pi.y, pi.z, P->inv_cell);
-    for (int a = 0; a < 3; a++)
-      for (int b = 0; b < 3; b++)
-        for (int c = 0; c < 3; c++) {
-          const uint32_t hb = ch.bucket(a, b, c, mask);
-          const uint32_t e1 = v.start[hb + 1];
-          for (uint32_t e = v.start[hb]; e < e1; e++) {
-            const uint32_t j = v.entries[e];
-            if (j == (uint32_t)i || j >= (uint32_t)v.S || cnt >= C_K) continue;
-            const float4 pj = v.pos[j];
-            const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-            const float lim = solid_rsum(v, P, i, j) + margin;
-            if (dot3(ex, ey, ez, ex, ey, ez) >= lim * lim) continue;
-            if (is_bonded(v, i, j)) continue;
-            v.clist[(size_t)i * C_K + cnt] = j;
-            cnt++;
-          }
-        }
-  }
-  v.ccount[i] = cnt;
+  b_collect_contacts(v, P, blockIdx.x);
 }
-
-// solidContacts, src/gpu/wgsl.js:562-585
 __global__ void __launch_bounds__(256) k_solid_contacts(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.S) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 pi = v.pos[i];
-  const float wi = pi.w;
-  float cx = 0.f, cy = 0.f, cz = 0.f;
-  const uint32_t n = v.ccount[i];
-  for (uint32_t k = 0; k < n; k++) {
-    const uint32_t j = v.clist[(size_t)i * C_K + k];
-    const float4 pj = v.pos[j];
-    const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-    const float rsum = solid_rsum(v, P, i, j);
-    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-    if (d2 >= rsum * rsum || d2 < 1e-12f) continue;
-    const float wsum = wi + pj.w;
-    if (wsum == 0.f) continue;
-    const float d = sqrtf(d2);
-    const float f = (rsum - d) / d * wi / wsum * 0.5f;
-    cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
-  }
-  v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+  b_solid_contacts(v, P, blockIdx.x);
 }
-
-// applySolidContacts, src/gpu/wgsl.js:587-596
 __global__ void __launch_bounds__(256) k_apply_solid_contacts(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.S) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float maxC = 0.5f * P->solid_radius;
-  const float4 dd = v.delta[i];
-  float dx = dd.x, dy = dd.y, dz = dd.z;
-  const float m2 = dot3(dx, dy, dz, dx, dy, dz);
-  if (m2 > maxC * maxC) {
-    const float f = maxC / sqrtf(m2);
-    dx = dx * f; dy = dy * f; dz = dz * f;
-  }
-  float4 p = v.pos[i];
-  p.x = p.x + dx; p.y = p.y + dy; p.z = p.z + dz;
-  v.pos[i] = p;
-  v.spos[v.slot[i]] = p;
+  b_apply_solid_contacts(v, P, blockIdx.x);
 }
-
-__device__ __forceinline__ void cross3(float ax, float ay, float az, float bx, float by, float bz,
-                                       float& x, float& y, float& z) {
-  x = ay * bz - az * by;
-  y = az * bx - ax * bz;
-  z = ax * by - ay * bx;
-}
-
-// solveTets, src/gpu/wgsl.js:423-468
 __global__ void __launch_bounds__(256) k_solve_tets(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.S) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const uint32_t* ids = v.tet_adj + v.S + 1;
-  float cx = 0.f, cy = 0.f, cz = 0.f;
-  for (uint32_t k = v.tet_adj[i]; k < v.tet_adj[i + 1]; k++) {
-    const uint32_t t = ids[k];
-    const uint32_t ia = v.tet_idx[4 * t], ib = v.tet_idx[4 * t + 1], ic = v.tet_idx[4 * t + 2],
-                   id = v.tet_idx[4 * t + 3];
-    const float V0 = v.tet_vol[t];
-    if (V0 <= 0.f) continue;
-    const float4 pa = v.pos[ia], pb = v.pos[ib], pc = v.pos[ic], pd = v.pos[id];
-    const float bax = pb.x - pa.x, bay = pb.y - pa.y, baz = pb.z - pa.z;
-    const float cax = pc.x - pa.x, cay = pc.y - pa.y, caz = pc.z - pa.z;
-    const float dax = pd.x - pa.x, day = pd.y - pa.y, daz = pd.z - pa.z;
-    float xx, xy, xz;
-    cross3(bax, bay, baz, cax, cay, caz, xx, xy, xz);
-    const float V = dot3(xx, xy, xz, dax, day, daz) / 6.0f;
-    const float Cv = V - V0;
-    float gbx, gby, gbz, gcx, gcy, gcz, gdx, gdy, gdz;
-    cross3(cax, cay, caz, dax, day, daz, gbx, gby, gbz);
-    gbx = gbx / 6.0f; gby = gby / 6.0f; gbz = gbz / 6.0f;
-    cross3(dax, day, daz, bax, bay, baz, gcx, gcy, gcz);
-    gcx = gcx / 6.0f; gcy = gcy / 6.0f; gcz = gcz / 6.0f;
-    cross3(bax, bay, baz, cax, cay, caz, gdx, gdy, gdz);
-    gdx = gdx / 6.0f; gdy = gdy / 6.0f; gdz = gdz / 6.0f;
-    const float gax = -((gbx + gcx) + gdx), gay = -((gby + gcy) + gdy), gaz = -((gbz + gcz) + gdz);
-    const float w = pa.w;
-    const float denom = w * (dot3(gax, gay, gaz, gax, gay, gaz) + dot3(gbx, gby, gbz, gbx, gby, gbz) +
-                             dot3(gcx, gcy, gcz, gcx, gcy, gcz) + dot3(gdx, gdy, gdz, gdx, gdy, gdz));
-    if (denom < 1e-12f) continue;
-    const float dl = -Cv / denom;
-    const uint32_t da = v.tet_adj[ia + 1] - v.tet_adj[ia], db = v.tet_adj[ib + 1] - v.tet_adj[ib];
-    const uint32_t dc = v.tet_adj[ic + 1] - v.tet_adj[ic], dd = v.tet_adj[id + 1] - v.tet_adj[id];
-    const uint32_t m1 = (da < db) ? db : da, m2 = (dc < dd) ? dd : dc;
-    uint32_t dm = (m1 < m2) ? m2 : m1;
-    if (dm < 1u) dm = 1u;
-    const float s = 1.0f / (float)dm;
-    float gx = gax, gy = gay, gz = gaz;
-    if ((uint32_t)i == ib) { gx = gbx; gy = gby; gz = gbz; }
-    else if ((uint32_t)i == ic) { gx = gcx; gy = gcy; gz = gcz; }
-    else if ((uint32_t)i == id) { gx = gdx; gy = gdy; gz = gdz; }
-    const float f = w * dl * s;
-    float c1x = gx * f, c1y = gy * f, c1z = gz * f;
-    const float cl2 = dot3(c1x, c1y, c1z, c1x, c1y, c1z);
-    const float lim = 0.5f * P->solid_radius;
-    if (cl2 > lim * lim) {
-      const float g = lim / sqrtf(cl2);
-      c1x = c1x * g; c1y = c1y * g; c1z = c1z * g;
-    }
-    cx = cx + c1x; cy = cy + c1y; cz = cz + c1z;
-  }
-  v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+  b_solve_tets(v, P, blockIdx.x);
 }
-
-// -------------------------------------------- bond update + contacts
-// Threads [0, nb) run bondUpdate (src/gpu/wgsl.js:383-404) on one constraint
-// each, threads [nb, nb+nt) run tetUpdate (src/gpu/wgsl.js:472-491), threads
-// [nb+nt, nb+nt+nc) run the solid↔fluid coupling gather `contacts`
-// (src/gpu/wgsl.js:609-646). All three read positions only; their outputs
-// (constraints, tets, delta) are disjoint.
-__device__ __forceinline__ void bond_update(const SimView& v, const DevParams* __restrict__ P, int ci) {
-  const uint4 c = v.cons[ci];
-  if (c.w == 0u) return;
-  const float4 pa = v.pos[c.x], pb = v.pos[c.y];
-  const float ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
-  const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
-  const float rest = __uint_as_float(c.z);
-  const bool tear = (P->tear_mode == 1) ? (d > rest * P->break_strain)
-                                        : (d > rest + P->tear_gap * 2.0f * P->solid_radius);
-  if (tear) {
-    v.cons[ci].w = 0u;
-    return;
-  }
-  const float strain = (d - rest) / rest;
-  float nr = rest;
-  if (fabsf(strain) > P->plastic_threshold) nr = rest + (d - rest) * P->plastic_rate;
-  if (P->plastic_clamp) {
-    const float r0 = lattice_rest(v, P->spacing, c.x, c.y);
-    nr = clampf(nr, 0.9f * r0, 1.25f * r0);
-  }
-  if (nr != rest) v.cons[ci].z = __float_as_uint(nr);
+__global__ void __launch_bounds__(256) k_bond_contacts(SimView v, const DevParams* __restrict__ P, int nb, int nt,
+                                                       int nb_pad, int nc) {
+  b_bond_contacts(v, P, nb, nt, nb_pad, nc, blockIdx.x);
 }
-
-__device__ __forceinline__ void tet_update(const SimView& v, const DevParams* __restrict__ P, int t) {
-  const float V0 = v.tet_vol[t];
-  if (V0 <= 0.f) return;
-  const float gap = P->tear_gap * 2.0f * P->solid_radius;
-  for (int p = 0; p < 3; p++)
-    for (int q = p + 1; q < 4; q++) {
-      const uint32_t a = v.tet_idx[4 * t + p], b = v.tet_idx[4 * t + q];
-      const float4 pa = v.pos[a], pb = v.pos[b];
-      const float ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
-      const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
-      if (d > lattice_rest(v, P->spacing, a, b) + gap) {
-        v.tet_vol[t] = -V0;
-        return;
-      }
-    }
+__global__ void __launch_bounds__(256) k_apply_bounds_vel(SimView v, const DevParams* __restrict__ P, int stage) {
+  b_apply_bounds_vel(v, P, stage, blockIdx.x);
 }
-
-// contacts for particle i, lane `lane` of its GL; every lane reaches the
-// shuffles. Fluid particles that no solid marked have no contact and skip the
-// walk (their correction is zero either way).
-__device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams* __restrict__ P, int i, int lane,
-                                              int nc) {
-  const bool act = i < nc && (v.flags[i] & F_ACTIVE);
-  const bool iSolid = i < v.S;
-  const bool walk = act && (iSolid || !P->use_mark || v.mark[i] != 0u);
-  float cx = 0.f, cy = 0.f, cz = 0.f, cnt = 0.f;
-  const float4 pi = walk ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  CellHash ch;
-  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  if (walk) {
-    const float wi = pi.w;
-    const float rs = P->solid_radius, rf = P->fluid_radius, scale = P->contact_scale;
-    // a solid meets the fluid part of each bucket, a fluid particle the solid
-    // part (fluid-fluid is DDR's job, solid-solid the contact cache's)
-    const float ri = iSolid ? rs : rf;
-    const float rsum = ri + (iSolid ? rf : rs);
-    const float4* __restrict__ spos = v.spos;
-    auto pair = [&](uint32_t e) {
-      const float4 pj = spos[e];
-      const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      if (d2 >= rsum * rsum || d2 < 1e-12f) return;
-      const float wsum = wi + pj.w;
-      if (wsum == 0.f) return;
-      const float d = sqrtf(d2);
-      const float f = (rsum - d) / d * wi / wsum * scale;
-      cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
-      cnt = cnt + 1.0f;
-    };
-    if (iSolid)
-      lane_slots<0>(v, ch, lane, pair);
-    else
-      lane_slots<1>(v, ch, lane, pair);
-  }
-  cx = lane_sum(cx);
-  cy = lane_sum(cy);
-  cz = lane_sum(cz);
-  cnt = lane_sum(cnt);
-  if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, cnt);
-}
-
-// nb_pad is nb + nt rounded up to a multiple of 32, so the contact threads
-// start on a warp boundary and whole warps reach lane_sum's shuffles.
-__global__ void __launch_bounds__(256) k_bond_contacts(SimView v, const DevParams* __restrict__ P,
-                                                       int nb, int nt, int nb_pad, int nc) {
-  const int t = UPBD_TID;
-  if (t < nb_pad) {
-    if (t < nb)
-      bond_update(v, P, t);
-    else if (t < nb + nt)
-      tet_update(v, P, t - nb);
-    return;
-  }
-  const int c = t - nb_pad;
-  contacts_lane(v, P, c / GL, c & (GL - 1), nc);
-}
-
-// -------------------------------- apply + bounds + velocity (per particle)
-// applyDeltaAll (src/gpu/wgsl.js:648-660), bounds (src/gpu/wgsl.js:663-697)
-// and velocityUpdate (src/gpu/wgsl.js:700-710): each touches only its own
-// particle, so one launch runs all three. stage 1/2/3 stops after the first,
-// second or third.
-__global__ void __launch_bounds__(256) k_apply_bounds_vel(SimView v, const DevParams* __restrict__ P,
-                                                          int stage) {
-  const int i = UPBD_TID;
-  if (i >= v.N) return;
-  uint32_t f = v.flags[i];
-  if (!(f & F_ACTIVE)) return;
-  const bool iSolid = i < v.S;
-  const float r = iSolid ? P->solid_radius : P->fluid_radius;
-  float4 p = v.pos[i];
-  // applyDeltaAll
-  {
-    const float4 dd = v.delta[i];
-    float dx = dd.x, dy = dd.y, dz = dd.z;
-    const float m2 = dot3(dx, dy, dz, dx, dy, dz);
-    if (m2 > r * r) {
-      const float g = r / sqrtf(m2);
-      dx = dx * g; dy = dy * g; dz = dz * g;
-    }
-    p.x = p.x + dx; p.y = p.y + dy; p.z = p.z + dz;
-  }
-  const uint32_t sl = v.slot[i];
-  if (stage < 2) {
-    v.pos[i] = p;
-    v.spos[sl] = p;
-    return;
-  }
-  // bounds
-  const float4 pv = v.prev[i];
-  float px = p.x, py = p.y, pz = p.z;
-  if (py < r) {
-    py = r;
-    const float mu = iSolid ? P->friction_solid : P->friction_fluid;
-    px = px - (px - pv.x) * mu;
-    pz = pz - (pz - pv.z) * mu;
-  }
-  if (py < P->wall_h + r) {
-    const float lim = r + P->wall_t;
-    const float wx = P->wall_x, wz = P->wall_z;
-    if (fabsf(fabsf(px) - wx) < lim) {
-      const float side = signf(px);
-      px = (fabsf(px) < wx) ? side * (wx - lim) : side * (wx + lim);
-    }
-    if (fabsf(fabsf(pz) - wz) < lim) {
-      const float side = signf(pz);
-      pz = (fabsf(pz) < wz) ? side * (wz - lim) : side * (wz + lim);
-    }
-  }
-  bool culled = false;
-  if (!iSolid) {
-    const float cr = P->cull_r;
-    if (py < -3.0f || px * px + pz * pz > cr * cr) {
-      v.flags[i] = 0u;
-      culled = true;
-    }
-  }
-  p.x = px; p.y = py; p.z = pz;
-  v.pos[i] = p;
-  v.spos[sl] = p;
-  if (stage < 3) return;
-  if (culled) {
-    // xsph still reads a culled neighbour's velocity (src/gpu/wgsl.js:761
-    // does not test its flag): its slot keeps the unchanged velocity
-    v.svel[sl] = v.vel[i];
-    return;
-  }
-  // velocityUpdate
-  const float h = P->h;
-  float vx = (p.x - pv.x) / h, vy = (p.y - pv.y) / h, vz = (p.z - pv.z) / h;
-  const float damp = iSolid ? P->damp_solid : P->damp_fluid;
-  const float g = mx(0.0f, 1.0f - damp * h);
-  vx = vx * g; vy = vy * g; vz = vz * g;
-  const float sp2 = dot3(vx, vy, vz, vx, vy, vz);
-  const float ms = P->max_speed;
-  if (sp2 > ms * ms) {
-    const float q = ms / sqrtf(sp2);
-    vx = vx * q; vy = vy * q; vz = vz * q;
-  }
-  if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) atomicOr(&v.scratch[SCR_HEALTH], 1u);
-  const float vw = v.vel[i].w;
-  const float4 nv = make_float4(vx, vy, vz, vw);
-  v.vel[i] = nv;
-  v.svel[sl] = nv;
-}
-
-// solidVisc, src/gpu/wgsl.js:717-735
 __global__ void __launch_bounds__(256) k_solid_visc(SimView v, const DevParams* __restrict__ P) {
-  const int i = UPBD_TID;
-  if (i >= v.S) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const uint32_t* ids = v.adj + v.S + 1;
-  float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
-  for (uint32_t k = v.adj[i]; k < v.adj[i + 1]; k++) {
-    const uint4 c = v.cons[ids[k]];
-    if (c.w == 0u) continue;
-    const uint32_t other = (c.x == (uint32_t)i) ? c.y : c.x;
-    const float4 vo = v.vel[other];
-    sx = sx + vo.x; sy = sy + vo.y; sz = sz + vo.z;
-    m = m + 1.0f;
-  }
-  const float4 vi = v.vel[i];
-  float vx = vi.x, vy = vi.y, vz = vi.z;
-  if (m > 0.f) {
-    const float mu = P->solid_viscosity;
-    vx = vx + mu * (sx / m - vx);
-    vy = vy + mu * (sy / m - vy);
-    vz = vz + mu * (sz / m - vz);
-  }
-  v.delta[i] = make_float4(vx, vy, vz, 0.f);
+  b_solid_visc(v, P, blockIdx.x);
 }
-
-// solidViscApply, src/gpu/wgsl.js:737-742
-__global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) {
-  const int i = UPBD_TID;
-  if (i >= v.S) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 d = v.delta[i];
-  const float w = v.vel[i].w;
-  v.vel[i] = make_float4(d.x, d.y, d.z, w);
-}
-
-// xsph, src/gpu/wgsl.js:745-771
-__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) {
-  const int t = UPBD_TID;
-  const int lane = threadIdx.x & (GL - 1);
-  const int i = v.S + t / GL;
-  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
-  float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
-  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  CellHash ch;
-  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  if (act) {
-    const float H = P->fluid_h, H2 = H * H;
-    const float4* __restrict__ spos = v.spos;
-    const float4* __restrict__ svel = v.svel;
-    const uint32_t myslot = v.slot[i];
-    lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-      const float4 pj = spos[e];
-      if (e == myslot) return;
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
-      const float4 vj = svel[e];
-      sx = sx + vj.x; sy = sy + vj.y; sz = sz + vj.z;
-      m = m + 1.0f;
-    });
-  }
-  sx = lane_sum(sx);
-  sy = lane_sum(sy);
-  sz = lane_sum(sz);
-  m = lane_sum(m);
-  if (act && lane == 0) {
-    const float4 vi = v.vel[i];
-    float vx = vi.x, vy = vi.y, vz = vi.z;
-    if (m > 0.f) {
-      const float mu = P->viscosity;
-      vx = vx + mu * (sx / m - vx);
-      vy = vy + mu * (sy / m - vy);
-      vz = vz + mu * (sz / m - vz);
-    }
-    v.delta[i] = make_float4(vx, vy, vz, m);
-  }
-}
-
-// xsphApply, src/gpu/wgsl.js:773-778
-__global__ void __launch_bounds__(256) k_xsph_apply(SimView v) {
-  const int i = v.S + (int)UPBD_TID;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 d = v.delta[i];
-  v.vel[i] = make_float4(d.x, d.y, d.z, 0.f);
-}
+__global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) { b_solid_visc_apply(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) { b_xsph(v, P, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_xsph_apply(SimView v) { b_xsph_apply(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_count_active(SimView v) { b_count_active(v, blockIdx.x, gridDim.x); }
 
 // ------------------------------------------------------------------ tools
 // Wedge cut over the constraint buffer (kernel shape of src/gpu/wgsl.js:804-823)
@@ -1073,32 +268,6 @@ __global__ void k_grab_release(SimView v) {
 __global__ void k_drain(SimView v) {
   const int i = v.S + (int)UPBD_TID;
   if (i < v.N) v.flags[i] = 0u;
-}
-
-// countActive (src/gpu/wgsl.js:874-879) with a last-block epilogue that
-// publishes the count and the health bits to mapped host memory.
-__global__ void __launch_bounds__(256) k_count_active(SimView v) {
-  const int i = v.S + (int)UPBD_TID;
-  uint32_t a = (i < v.N && (v.flags[i] & F_ACTIVE)) ? 1u : 0u;
-  a = __reduce_add_sync(0xffffffffu, a);
-  __shared__ uint32_t s_sum;
-  if (threadIdx.x == 0) s_sum = 0;
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0 && a) atomicAdd(&s_sum, a);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (s_sum) atomicAdd(&v.scratch[SCR_ACTIVE], s_sum);
-    __threadfence();
-    const uint32_t done = atomicAdd(&v.scratch[SCR_DONE], 1u);
-    if (done == gridDim.x - 1) {
-      __threadfence();
-      const uint32_t total = atomicExch(&v.scratch[SCR_ACTIVE], 0u);
-      v.scratch[SCR_DONE] = 0u;
-      volatile uint32_t* hm = v.host_mapped;
-      hm[HM_ACTIVE] = total;
-      hm[HM_HEALTH] = atomicOr(&v.scratch[SCR_HEALTH], 0u);
-    }
-  }
 }
 
 }  // namespace upbd
