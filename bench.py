@@ -210,6 +210,130 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, stream, hbm: float) -> dict:
+    """The uneven batch: 256 independent scenes (body dim uniform in 6..20,
+    fluid log-uniform in [2k, 65k], one seed each) stepped together, one
+    persistent launch per pass; grid shape autotuned first. The state (~5 GB)
+    is far larger than L2, so no flush is needed between frames. Beside it,
+    the plain per-scene path (one single-scene handle per scene, each frame
+    its own captured graph) on a sample of the same scenes."""
+    import torch
+    from fluidphysics_b200 import _lib as L
+    from fluidphysics_b200 import batch as B
+    from fluidphysics_b200.sim import sim_from_scene
+    scs = B.batch_scenes(args.batched_scenes)
+    dt, nsub = 1 / 60, 5
+    b = B.Batch(max_scenes=max(256, len(scs)))
+    b.set_stream(stream.cuda_stream)
+    ids = [b.add_scene(sc) for sc in scs]
+    for _ in range(3):
+        b.step(dt, nsub)
+    b.sync()
+    best, table = B.autotune(b, dict(zip(ids, scs)), dt, nsub, frames=3, block_threads=(128, 256),
+                             ctas_per_sm=(8, 16), warm_frames=1)
+    for _ in range(3):
+        b.step(dt, nsub)
+    b.sync()
+    K = args.batched_frames
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.launches
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        b.step(dt, nsub)
+    e1.record(stream)
+    b.sync()
+    ms = e0.elapsed_time(e1)
+    launches = b.launches - l0
+    active, B_sub = 0, 0
+    for i in ids:
+        si, af = b.scene_info(i), b.active_count(i)
+        active += si.solid_n + af
+        # the substep's algorithmic bytes (the unit of account of the plain line)
+        B_sub += (240 * (si.solid_n + af) + 200 * af + 8 * si.table_size
+                  + si.solid_iters * (84 * si.solid_n + 24 * si.num_cons) + 20 * si.num_cons)
+    value = active * nsub * K / (ms / 1e3)
+    step_gbs = B_sub * nsub * K / (ms / 1e3) / 1e9
+    # per-kernel shares of one eager frame
+    msk, ln = b.profile_frame(dt, nsub)
+    names = [(b.lib.upbd_kernel_name(k) or b"").decode() for k in range(L.KERNEL_KINDS)]
+    shares = {names[k]: {"share": round(float(msk[k] / msk.sum()), 4),
+                         "avg_us": round(float(msk[k] * 1e3 / ln[k]), 1), "launches_per_frame": int(ln[k])}
+              for k in np.argsort(-msk) if ln[k]}
+    info = b.info()
+    b.close()
+    # plain per-scene path on every 8th scene
+    sample = scs[::8]
+    pp_units, pp_ms = 0.0, 0.0
+    for sc in sample:
+        sim = sim_from_scene(sc)
+        sim.set_stream(stream.cuda_stream)
+        for _ in range(3):
+            sim.step(dt, nsub)
+        sim.sync()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(20):
+            sim.step(dt, nsub)
+        a1.record(stream)
+        sim.sync()
+        pp_ms += a0.elapsed_time(a1)
+        pp_units += (sc.solid_n + sim.active_count()) * nsub * 20
+        sim.close()
+    pp = pp_units / (pp_ms / 1e3)
+    return {
+        "value": value, "unit": UNIT, "frames": K, "scenes": len(scs), "particles": int(info.particles),
+        "active_particles": int(active), "ms_per_frame": ms / K, "gpu_launches": int(launches),
+        "workload": f"{len(scs)} scenes, body dim U{{6..20}}, fluid floor(2^U(11,16)), deriveOpts at 30 mm, "
+                    "seeds 1000+k, 5 substeps x 3 iterations, frames 7.. of each scene",
+        "l2": "state ~{:.1f} GB > L2 (no flush)".format(info.bytes_in_use / 1e9),
+        "tuning": {"block_threads": best.block_threads, "ctas_per_sm": best.ctas_per_sm,
+                   "cell_scale": best.cell_scale,
+                   "candidates_ms": [[t.block_threads, t.ctas_per_sm, round(t.ms_per_frame, 2)] for t in table]},
+        "kernels": shares,
+        "step_achieved_gbs": step_gbs, "step_frac": step_gbs / hbm,
+        "plain_per_scene": {"value": pp, "unit": UNIT,
+                            "sample": f"{len(sample)} of the scenes (every 8th), each its own single-scene "
+                                      "handle, 20 graph frames after 3 warm-up frames"},
+        "speedup_vs_plain_per_scene": value / pp,
+    }
+
+
+def run_served(args, batched: dict | None) -> dict:
+    """The served stream: Poisson arrivals at 200 scenes/s for
+    --served-window seconds; each request a scene of 1k-262k particles (body
+    fraction 0-30 %) asking for 1-60 frames; admitted by a 150 GB HBM budget,
+    resident between frames, stepped in continuous batches."""
+    from fluidphysics_b200 import server as SV
+    reqs = SV.served_requests(window_s=args.served_window, rate=200.0, seed=5)
+    bt, cps = (256, 8)
+    if batched:
+        bt, cps = batched["tuning"]["block_threads"], batched["tuning"]["ctas_per_sm"]
+    offered = sum(r.scene.total * r.frames * 5 for r in reqs) / args.served_window
+    with SV.Server(hbm_budget=150 * 10**9, max_scenes=4096, block_threads=bt, ctas_per_sm=cps,
+                   builders=8) as srv:
+        for r in reqs:
+            srv.submit(r.scene, r.frames, r.arrival_s)
+        srv.run(900)
+        st = srv.stats()
+    return {
+        "value": st["particle_substeps"] / st["wall_s"], "unit": UNIT,
+        "p50_frame_ms": st["frame_ms_p50"], "p99_frame_ms": st["frame_ms_p99"],
+        "p90_frame_ms": st["frame_ms_p90"], "mean_frame_ms": st["frame_ms_mean"], "max_frame_ms": st["frame_ms_max"],
+        "p50_wait_ms": st["wait_ms_p50"], "p99_wait_ms": st["wait_ms_p99"],
+        "p50_batch_frame_ms": st["batch_ms_p50"], "p99_batch_frame_ms": st["batch_ms_p99"],
+        "requests": st["submitted"], "completed": st["completed"], "rejected": st["rejected"],
+        "scene_frames": st["scene_frames"], "batched_frames": st["batch_frames"],
+        "mean_live_scenes": st["mean_scenes"], "peak_live_scenes": st["peak_scenes"],
+        "peak_bytes": st["peak_bytes"], "wall_s": st["wall_s"], "device_busy_s": st["device_s"],
+        "offered_particle_substeps_per_s": offered,
+        "workload": f"Poisson(200/s) arrivals for {args.served_window} s (seed 5); total particles "
+                    "log-uniform [1k, 262k], body fraction U(0, 0.3), frames U{1..60}; HBM budget 150 GB",
+        "latency": "frame latency = completion of the frame minus the time it could first run (arrival "
+                   "for a request's first frame, so queueing is included), server wall clock",
+    }
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -222,6 +346,11 @@ def main() -> None:
                     help="frames stepped from the initial state before the per-kernel profile")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batched-frames", type=int, default=300,
+                    help="timed frames of the 256-scene batch (0 skips the batched line)")
+    ap.add_argument("--batched-scenes", type=int, default=256)
+    ap.add_argument("--served-window", type=float, default=2.0,
+                    help="seconds of Poisson arrivals served (0 skips the served line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -389,6 +518,16 @@ def main() -> None:
     roofline["step_achieved_gbs"] = step_gbs
     roofline["step_frac"] = step_gbs / hbm
 
+    sim.close()
+    batched = run_batched(args, stream, hbm) if args.batched_frames > 0 else None
+    served = run_served(args, batched) if args.served_window > 0 else None
+    if pg:
+        for key, obj in (("batched", batched), ("served", served)):
+            if obj and obj.get("value"):
+                t = torch.tensor([obj["value"]], device="cuda", dtype=torch.float64)
+                pg.all_reduce(t, op=pg.ReduceOp.SUM)  # replicas: whole-job rate
+                obj["value"] = float(t.item())
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -415,9 +554,10 @@ def main() -> None:
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clk,
+            "batched": batched,
+            "served": served,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

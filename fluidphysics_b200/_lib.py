@@ -90,6 +90,39 @@ class BatchInfo(C.Structure):
     ]
 
 
+class ServerDesc(C.Structure):
+    """upbd_server_desc (include/upbd_server.h)."""
+    _fields_ = [("batch", BatchDesc), ("dt", C.c_double), ("substeps", C.c_int32), ("builders", C.c_int32),
+                ("keep_results", C.c_int32), ("reserved", C.c_int32 * 9)]
+
+
+class Request(C.Structure):
+    """upbd_request (include/upbd_server.h)."""
+    _fields_ = [("desc", SceneDesc), ("params", Params), ("frames", C.c_int32), ("n_fluid", C.c_int32),
+                ("fluid_mass", C.c_double), ("arrival_s", C.c_double),
+                ("fluid_pos3", C.POINTER(C.c_float)), ("fluid_vel3", C.POINTER(C.c_float)),
+                ("reserved", C.c_int32 * 8)]
+
+
+class RequestResult(C.Structure):
+    """upbd_request_result (include/upbd_server.h)."""
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("frames_done", C.c_int32), ("slots", C.c_int32),
+                ("arrival_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
+                ("frame_ms_max", C.c_double), ("reserved", C.c_int32 * 8)]
+
+
+class ServerStats(C.Structure):
+    """upbd_server_stats (include/upbd_server.h)."""
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("rejected", C.c_int64), ("scene_frames", C.c_int64), ("batch_frames", C.c_int64),
+                ("particle_substeps", C.c_double), ("wall_s", C.c_double), ("device_s", C.c_double),
+                ("frame_ms_p50", C.c_double), ("frame_ms_p90", C.c_double), ("frame_ms_p99", C.c_double),
+                ("frame_ms_max", C.c_double), ("frame_ms_mean", C.c_double), ("wait_ms_p50", C.c_double),
+                ("wait_ms_p99", C.c_double), ("batch_ms_p50", C.c_double), ("batch_ms_p99", C.c_double),
+                ("mean_scenes", C.c_double), ("peak_scenes", C.c_int32), ("reserved0", C.c_int32),
+                ("peak_bytes", C.c_uint64), ("reserved", C.c_double * 8)]
+
+
 # (name, restype, argtypes)
 _P = C.c_void_p
 _D3 = C.POINTER(C.c_double)
@@ -161,6 +194,15 @@ _SIGS = [
     ("upbd_batch_scene_info", C.c_int, [_P, C.c_int32, C.POINTER(Info)]),
     ("upbd_batch_active_count", C.c_int, [_P, C.c_int32, _U]),
     ("upbd_batch_profile_frame", C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(C.c_double), _U]),
+    # frame server (include/upbd_server.h)
+    ("upbd_server_default_desc", C.c_int, [C.POINTER(ServerDesc)]),
+    ("upbd_server_create", C.c_int, [C.POINTER(ServerDesc), C.POINTER(_P)]),
+    ("upbd_server_destroy", C.c_int, [_P]),
+    ("upbd_server_last_error", C.c_char_p, [_P]),
+    ("upbd_server_submit", C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    ("upbd_server_run", C.c_int, [_P, C.c_double]),
+    ("upbd_server_get_stats", C.c_int, [_P, C.POINTER(ServerStats)]),
+    ("upbd_server_result", C.c_int, [_P, C.c_int64, C.POINTER(RequestResult), _F, _U]),
 ]
 KERNEL_KINDS = 32
 

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
           "-I", str(INCLUDE), "-Xptxas", "-warn-spills"]
 
-SOURCES = ["upbd.cu", "upbd_scene.cu", "upbd_batch.cu"]
+SOURCES = ["upbd.cu", "upbd_scene.cu", "upbd_batch.cu", "upbd_server.cu"]
 TARGETS = {
     "libupbd.so": SOURCES,
     "libupbd_parity.so": SOURCES,

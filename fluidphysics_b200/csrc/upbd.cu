@@ -181,7 +181,7 @@ int launch_substep(upbd_sim* s, int last) {
   L += 4;
   UPBD_KCK(s);
   if (last < UPBD_PASS_DENSITY) return UPBD_OK;
-  const long long fl = (long long)v.F * GL;  // lane-parallel fluid gathers
+  const long long fl = (long long)v.N * GL;  // lane-parallel gathers over the slots
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_DISP) return UPBD_OK;
@@ -253,7 +253,7 @@ int launch_substep(upbd_sim* s, int last) {
     L += 2;
   }
   if (last < UPBD_PASS_XSPH) return UPBD_OK;
-  PROF(s, K_XSPH, k_xsph<<<blocks_for((long long)v.F * GL), 256, 0, st>>>(v, P));
+  PROF(s, K_XSPH, k_xsph<<<blocks_for((long long)v.N * GL), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_XSPH_APPLY) return UPBD_OK;
   PROF(s, K_XSPH_APPLY, k_xsph_apply<<<blocks_for(v.F), 256, 0, st>>>(v));

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/upbd_batch.h"
+#include "upbd_batch_internal.h"
 #include "upbd_kinds.h"
 #include "upbd_passes.cuh"
 #include "upbd_scene.h"
@@ -38,7 +39,7 @@ enum Domain {
   D_N,        // particles (integrate/count, rankfix, apply+bounds+velocity)
   D_TILES,    // scan tiles of the bucket table (SCAN_THREADS per block)
   D_SCATTER,  // max(particles, scan tiles)
-  D_FGL,      // GL lanes per fluid particle (density, displacement, xsph)
+  D_FGL,      // GL lanes per grid slot (density, displacement, xsph)
   D_F,        // fluid particles (apply, xsph apply, active count)
   D_SOLVE0,   // solve lanes rounded to warps + fluid (first iteration)
   D_SOLVE,    // solve lanes rounded to warps
@@ -182,7 +183,7 @@ void scene_blocks(const SimView& v, bool tets, int bt, uint32_t out[NUM_DOMAINS]
   out[D_N] = ceil_div(v.N, bt);
   out[D_TILES] = (uint32_t)std::max(v.num_tiles, 1);
   out[D_SCATTER] = ceil_div(std::max(v.N, v.num_tiles), bt);
-  out[D_FGL] = ceil_div((long long)v.F * GL, bt);
+  out[D_FGL] = ceil_div((long long)v.N * GL, bt);
   out[D_F] = ceil_div(v.F, bt);
   out[D_SOLVE0] = ceil_div((long long)sp + v.F, bt);
   out[D_SOLVE] = ceil_div(sp, bt);
@@ -522,6 +523,70 @@ BScene* find(upbd_batch* b, int32_t id) {
 
 }  // namespace
 
+namespace upbd {
+
+size_t prepared_bytes(const PreparedScene& ps) {
+  SimView v;
+  return layout_scene(ps.desc, *ps.lat, v).bytes;
+}
+
+int batch_add_prepared(upbd_batch* b, const PreparedScene& ps, int32_t* id) {
+  if (!b || !id || !ps.lat) return bfail(b, UPBD_ERR_INVALID, "null argument");
+  const upbd_scene_desc& d = ps.desc;
+  if (d.solid_iters != b->desc.solid_iters || d.features != b->desc.features)
+    return bfail(b, UPBD_ERR_INVALID, "scene solid_iters/features differ from the batch's");
+  if (b->free_hm.empty()) return bfail(b, UPBD_ERR_CAPACITY, "scene table is full");
+  cudaSetDevice(b->device);
+  BScene sc;
+  const SceneLayout L = layout_scene(d, *ps.lat, sc.v);
+  if (b->desc.hbm_budget && b->in_use + L.bytes > b->desc.hbm_budget)
+    return bfail(b, UPBD_ERR_CAPACITY, "scene does not fit the HBM budget");
+  sc.mem = b->pool.alloc(L.bytes);
+  if (!sc.mem) return bfail(b, UPBD_ERR_OOM, "device memory for the scene is not available");
+  sc.bytes = L.bytes;
+  DevParams* unused = nullptr;
+  bind_scene(L, sc.mem, sc.v, &unused);
+  sc.hm_slot = b->free_hm.back();
+  sc.v.host_mapped = b->dmapped + (size_t)sc.hm_slot * HM_WORDS;
+  cudaStream_t st = b->stream;
+  cudaError_t e = cudaMemsetAsync(sc.mem, 0, sc.bytes, st);
+  if (e == cudaSuccess) e = upload_prepared(ps, sc.v, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    b->pool.free(sc.mem, sc.bytes);
+    return bfail(b, UPBD_ERR_CUDA, std::string("scene upload: ") + cudaGetErrorString(e));
+  }
+  b->free_hm.pop_back();
+  std::memset(b->hmapped + (size_t)sc.hm_slot * HM_WORDS, 0, HM_WORDS * 4);
+  sc.id = b->next_id++;
+  sc.desc = d;
+  sc.prm = ps.prm;
+  fill_dev_params(ps.prm, d, sc.hp);
+  sc.hp.grab_lattice = 0xffff;
+  sc.init_cons = ps.lat->cons;
+  b->in_use += sc.bytes;
+  b->particles += sc.v.N;
+  b->solids += sc.v.S;
+  *id = sc.id;
+  b->scenes.emplace(sc.id, std::move(sc));
+  b->dirty = true;
+  return UPBD_OK;
+}
+
+cudaStream_t batch_stream(upbd_batch* b) { return b ? b->stream : nullptr; }
+
+bool batch_scene_counters(upbd_batch* b, int32_t id, uint32_t* active, uint32_t* health, int32_t* solids) {
+  BScene* sc = find(b, id);
+  if (!sc) return false;
+  const volatile uint32_t* hm = b->hmapped + (size_t)sc->hm_slot * HM_WORDS;
+  if (active) *active = hm[HM_ACTIVE];
+  if (health) *health = hm[HM_HEALTH];
+  if (solids) *solids = sc->v.S;
+  return true;
+}
+
+}  // namespace upbd
+
 extern "C" {
 
 int upbd_batch_default_desc(upbd_batch_desc* d) {
@@ -544,10 +609,8 @@ int upbd_batch_scene_bytes(const upbd_scene_desc* d, uint64_t* bytes) {
   upbd_params p;
   upbd_default_params(&p);
   if (const char* why = check_desc(d, &p)) return bfail(nullptr, UPBD_ERR_INVALID, why);
-  HostScene hs;
-  build_scene(*d, hs);
   SimView v;
-  *bytes = layout_scene(*d, hs, v).bytes;
+  *bytes = layout_scene(*d, *lattice_of(*d), v).bytes;
   return UPBD_OK;
 }
 
@@ -641,75 +704,11 @@ int upbd_batch_get_info(upbd_batch* b, upbd_batch_info* info) {
 int upbd_batch_add_scene(upbd_batch* b, const upbd_scene_desc* d, const upbd_params* p, int32_t n_fluid,
                          const float* fluid_pos3, const float* fluid_vel3, double fluid_mass, int32_t* id) {
   if (!b || !d || !p || !id) return bfail(b, UPBD_ERR_INVALID, "null argument");
-  if (const char* why = check_desc(d, p)) return bfail(b, UPBD_ERR_INVALID, why);
-  if (d->solid_iters != b->desc.solid_iters || d->features != b->desc.features)
-    return bfail(b, UPBD_ERR_INVALID, "scene solid_iters/features differ from the batch's");
   if (n_fluid < 0 || n_fluid > d->max_fluid) return bfail(b, UPBD_ERR_CAPACITY, "n_fluid exceeds max_fluid");
-  if (n_fluid > 0 && (!fluid_pos3 || !(fluid_mass > 0)))
-    return bfail(b, UPBD_ERR_INVALID, "fluid positions and a positive mass are required");
-  if (b->free_hm.empty()) return bfail(b, UPBD_ERR_CAPACITY, "scene table is full");
-  cudaSetDevice(b->device);
-  BScene sc;
-  HostScene hs;
-  build_scene(*d, hs);
-  const SceneLayout L = layout_scene(*d, hs, sc.v);
-  if (b->desc.hbm_budget && b->in_use + L.bytes > b->desc.hbm_budget)
-    return bfail(b, UPBD_ERR_CAPACITY, "scene does not fit the HBM budget");
-  sc.mem = b->pool.alloc(L.bytes);
-  if (!sc.mem) return bfail(b, UPBD_ERR_OOM, "device memory for the scene is not available");
-  sc.bytes = L.bytes;
-  DevParams* unused = nullptr;
-  bind_scene(L, sc.mem, sc.v, &unused);
-  sc.hm_slot = b->free_hm.back();
-  sc.v.host_mapped = b->dmapped + (size_t)sc.hm_slot * HM_WORDS;
-  // fluid particles as upbd_emit_particles places them (slots S.., inverse
-  // mass 1/mass, prev.w = 0, active)
-  const int S = sc.v.S;
-  std::vector<float4> prev(hs.pos);
-  std::vector<float4> vel;
-  std::vector<uint32_t> flags;
-  const float inv_mass = n_fluid > 0 ? (float)(1 / fluid_mass) : 0.f;
-  for (int k = 0; k < n_fluid; k++) {
-    const float x = fluid_pos3[3 * k], y = fluid_pos3[3 * k + 1], z = fluid_pos3[3 * k + 2];
-    hs.pos[S + k] = make_float4(x, y, z, inv_mass);
-    prev[S + k] = make_float4(x, y, z, 0.f);
-  }
-  cudaStream_t st = b->stream;
-  cudaError_t e = cudaMemsetAsync(sc.mem, 0, sc.bytes, st);
-  if (e == cudaSuccess) e = upload_scene(hs, sc.v, st);
-  if (e == cudaSuccess && n_fluid > 0) {
-    e = cudaMemcpyAsync(sc.v.prev + S, prev.data() + S, (size_t)n_fluid * 16, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && fluid_vel3) {
-      vel.resize(n_fluid);
-      for (int k = 0; k < n_fluid; k++)
-        vel[k] = make_float4(fluid_vel3[3 * k], fluid_vel3[3 * k + 1], fluid_vel3[3 * k + 2], 0.f);
-      e = cudaMemcpyAsync(sc.v.vel + S, vel.data(), (size_t)n_fluid * 16, cudaMemcpyHostToDevice, st);
-    }
-    if (e == cudaSuccess) {
-      flags.assign(n_fluid, F_ACTIVE);
-      e = cudaMemcpyAsync(sc.v.flags + S, flags.data(), (size_t)n_fluid * 4, cudaMemcpyHostToDevice, st);
-    }
-  }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors end here
-  if (e != cudaSuccess) {
-    b->pool.free(sc.mem, sc.bytes);
-    return bfail(b, UPBD_ERR_CUDA, std::string("scene upload: ") + cudaGetErrorString(e));
-  }
-  b->free_hm.pop_back();
-  std::memset(b->hmapped + (size_t)sc.hm_slot * HM_WORDS, 0, HM_WORDS * 4);
-  sc.id = b->next_id++;
-  sc.desc = *d;
-  sc.prm = *p;
-  fill_dev_params(*p, *d, sc.hp);
-  sc.hp.grab_lattice = 0xffff;
-  sc.init_cons = std::move(hs.cons);
-  b->in_use += sc.bytes;
-  b->particles += sc.v.N;
-  b->solids += sc.v.S;
-  *id = sc.id;
-  b->scenes.emplace(sc.id, std::move(sc));
-  b->dirty = true;
-  return UPBD_OK;
+  PreparedScene ps;
+  if (const char* why = prepare_scene(*d, *p, n_fluid, fluid_pos3, fluid_vel3, fluid_mass, ps))
+    return bfail(b, UPBD_ERR_INVALID, why);
+  return batch_add_prepared(b, ps, id);
 }
 
 int upbd_batch_remove_scene(upbd_batch* b, int32_t id) {

@@ -93,9 +93,9 @@ struct SimView {
   // precede solids: fend[h] splits bucket h into [start[h], fend[h]) fluid and
   // [fend[h], start[h+1]) solid.
   uint32_t* fend;
-  // Density-pass neighbour lists: lane g = (i - S)*GL + l of fluid particle i
-  // records the slots of its in-range fluid neighbours, in walk order, at
-  // nbr[c * F*GL + g] (c < NL), and their number in ncount[g].
+  // Density-pass neighbour lists: lane g = e*GL + l of the fluid particle at
+  // slot e records the slots of its in-range fluid neighbours, in walk order,
+  // at nbr[c * N*GL + g] (c < NL), and their number in ncount[g].
   uint32_t* nbr;
   uint32_t* ncount;
   const uint32_t* adj_other;  // CSR-parallel: the other endpoint of constraint ids[k]

@@ -176,24 +176,36 @@ __device__ __forceinline__ void b_rankfix(const SimView& v, uint32_t vb) {
 // ------------------------------------------------------------------ fluid
 // The neighbour gathers run GL lanes per particle (see lane_slots): a warp
 // holds 32/GL particles, every lane reaches the shuffles, and lane 0 writes.
+// Groups take the particles in slot order (group g: the particle at slot g of
+// this substep's grid, entries[g]): the particles of one bucket sit in
+// consecutive slots and share their 27 neighbour buckets, so a warp's
+// candidate loads mostly hit L1. A particle's own arithmetic does not depend
+// on which group runs it. Groups whose slot holds a solid, or lies past the
+// active count start[T], have no work.
+__device__ __forceinline__ void slot_group(const SimView& v, uint32_t t, uint32_t& e0, uint32_t& i, bool& fluid) {
+  e0 = t / GL;
+  const uint32_t nact = __ldg(&v.start[v.T]);
+  i = (e0 < nact) ? v.entries[e0] : 0u;
+  fluid = e0 < nact && i >= (uint32_t)v.S;
+}
 
-// fluidDensity, src/gpu/wgsl.js:254-279
+// fluidDensity, src/gpu/wgsl.js:254-279. Every grid entry is active (the
+// grid is built from the active particles of this substep, before bounds).
 __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
-  const int t = UPBD_VTID;
+  const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GL - 1);
-  const int i = v.S + t / GL;
-  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
+  uint32_t myslot, i;
+  bool act;
+  slot_group(v, t, myslot, i, act);
   float rho = 0.f, rhoNear = 0.f;
-  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  uint32_t myslot = 0;
   if (act) {
     const float H = P->fluid_h, H2 = H * H;
     const float4* __restrict__ spos = v.spos;
-    myslot = v.slot[i];
-    const uint32_t FG = (uint32_t)v.F * GL;
-    const uint32_t g = (uint32_t)(i - v.S) * GL + lane;
+    const uint32_t NG = (uint32_t)v.N * GL;
+    const uint32_t g = myslot * GL + lane;
     uint32_t* __restrict__ nbr = v.nbr + g;
     uint32_t cnt = 0;
     lane_slots<0>(v, ch, lane, [&](uint32_t e) {
@@ -205,7 +217,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
       const float q = 1.0f - sqrtf(d2) / H;
       rho = rho + q * q;
       rhoNear = rhoNear + q * q * q;
-      if (cnt < NL) nbr[cnt * FG] = e;  // for fluidDisp, same positions
+      if (cnt < NL) nbr[cnt * NG] = e;  // for fluidDisp, same positions
       cnt++;
     });
     v.ncount[g] = cnt;
@@ -219,24 +231,25 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   }
 }
 
-// fluidDisp, src/gpu/wgsl.js:281-316
+// fluidDisp, src/gpu/wgsl.js:281-316 (slot-ordered groups, as b_density)
 __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
-  const int t = UPBD_VTID;
+  const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GL - 1);
-  const int i = v.S + t / GL;
-  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
+  uint32_t myslot, i;
+  bool act;
+  slot_group(v, t, myslot, i, act);
   const float H = P->fluid_h, H2 = H * H;
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const uint32_t FG = (uint32_t)v.F * GL;
-  const uint32_t g = (uint32_t)(i - v.S) * GL + lane;
+  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t NG = (uint32_t)v.N * GL;
+  const uint32_t g = myslot * GL + lane;
   const uint32_t cnt = act ? v.ncount[g] : 0u;
   CellHash ch;
   if (__any_sync(0xffffffffu, cnt > NL)) group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
   if (act) {
     const float maxPair = 0.05f * H;
     const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
-    const float2 di = v.density[i];
+    const float2 di = v.sdens[myslot];
     const float Pi = k * (di.x - rho0);
     const float PNi = kn * di.y;
     const float4* __restrict__ spos = v.spos;
@@ -260,9 +273,8 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
     // positions and in walk order; a lane whose list overflowed walks again
     if (cnt <= NL) {
       const uint32_t* __restrict__ nbr = v.nbr + g;
-      for (uint32_t c = 0; c < cnt; c++) pair(__ldg(&nbr[c * FG]));
+      for (uint32_t c = 0; c < cnt; c++) pair(__ldg(&nbr[c * NG]));
     } else {
-      const uint32_t myslot = v.slot[i];
       lane_slots<0>(v, ch, lane, [&](uint32_t e) {
         if (e != myslot) pair(e);
       });
@@ -822,21 +834,25 @@ __device__ __forceinline__ void b_solid_visc_apply(const SimView& v, uint32_t vb
   v.vel[i] = make_float4(d.x, d.y, d.z, w);
 }
 
-// xsph, src/gpu/wgsl.js:745-771
+// xsph, src/gpu/wgsl.js:745-771 (slot-ordered groups, as b_density). The
+// grid still holds the particles bounds culled this substep: they are
+// neighbours (the reference does not test their flag) but have no pass of
+// their own.
 __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
-  const int t = UPBD_VTID;
+  const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GL - 1);
-  const int i = v.S + t / GL;
-  const bool act = i < v.N && (v.flags[i] & F_ACTIVE);
+  uint32_t myslot, i;
+  bool fluid;
+  slot_group(v, t, myslot, i, fluid);
+  const bool act = fluid && (v.flags[i] & F_ACTIVE);
   float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
-  const float4 pi = act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
   if (act) {
     const float H = P->fluid_h, H2 = H * H;
     const float4* __restrict__ spos = v.spos;
     const float4* __restrict__ svel = v.svel;
-    const uint32_t myslot = v.slot[i];
     lane_slots<0>(v, ch, lane, [&](uint32_t e) {
       const float4 pj = spos[e];
       if (e == myslot) return;

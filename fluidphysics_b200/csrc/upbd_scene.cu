@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace upbd {
 
@@ -150,7 +152,7 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   v.dim1 = d.solid_dim;
   v.dim2 = d.solid_dim2;
   v.F = d.max_fluid;
-  v.N = hs.N;
+  v.N = hs.S + d.max_fluid;
   v.C = (int)hs.cons.size();
   v.NT = (int)hs.tet_vol.size();
   v.T = d.table_size;
@@ -182,8 +184,8 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.svel = cv.take<float4>(v.N);
   L.slot = cv.take<uint32_t>(v.N);
   L.fend = cv.take<uint32_t>(v.T);
-  L.nbr = cv.take<uint32_t>(std::max<size_t>((size_t)v.F * GL * NL, 1));
-  L.ncount = cv.take<uint32_t>(std::max<size_t>((size_t)v.F * GL, 1));
+  L.nbr = cv.take<uint32_t>(std::max<size_t>((size_t)v.N * GL * NL, 1));
+  L.ncount = cv.take<uint32_t>(std::max<size_t>((size_t)v.N * GL, 1));
   L.aoth = cv.take<uint32_t>(std::max<size_t>(hs.adj_other.size(), 1));
   L.ascl = cv.take<float>(std::max<size_t>(hs.adj_scale.size(), 1));
   L.ccount = cv.take<uint32_t>(scc ? std::max(v.S, 1) : 1);
@@ -252,6 +254,95 @@ cudaError_t upload_scene(const HostScene& hs, const SimView& v, cudaStream_t st)
     std::vector<uint32_t> f((size_t)v.S, F_ACTIVE);
     e = cudaMemcpyAsync(v.flags, f.data(), (size_t)v.S * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // f is a stack buffer
+  }
+  return e;
+}
+
+namespace {
+struct LatticeKey {
+  int dim1, dim2;
+  double spacing, solid_mass, c1[3], c2[3];
+  bool operator<(const LatticeKey& o) const { return std::memcmp(this, &o, sizeof(*this)) < 0; }
+};
+std::mutex g_lat_mu;
+std::map<LatticeKey, std::shared_ptr<const HostScene>> g_lat;
+constexpr size_t kLatticeCacheMax = 128;
+}  // namespace
+
+std::shared_ptr<const HostScene> lattice_of(const upbd_scene_desc& d) {
+  LatticeKey k;
+  std::memset(&k, 0, sizeof(k));
+  k.dim1 = d.solid_dim;
+  k.dim2 = d.solid_dim2;
+  k.spacing = d.spacing;
+  k.solid_mass = d.solid_mass;
+  for (int i = 0; i < 3; i++) {
+    k.c1[i] = d.cube_center[i];
+    k.c2[i] = d.solid_dim2 > 0 ? d.cube2_center[i] : 0.0;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_lat_mu);
+    auto it = g_lat.find(k);
+    if (it != g_lat.end()) return it->second;
+  }
+  upbd_scene_desc ld = d;
+  ld.max_fluid = 0;
+  auto hs = std::make_shared<HostScene>();
+  build_scene(ld, *hs);
+  std::lock_guard<std::mutex> lk(g_lat_mu);
+  if (g_lat.size() >= kLatticeCacheMax) g_lat.clear();
+  return g_lat.emplace(k, std::move(hs)).first->second;
+}
+
+const char* prepare_scene(const upbd_scene_desc& d, const upbd_params& p, int n_fluid, const float* pos3,
+                          const float* vel3, double mass, PreparedScene& out) {
+  if (const char* why = check_desc(&d, &p)) return why;
+  if (n_fluid < 0 || n_fluid > d.max_fluid) return "n_fluid exceeds max_fluid";
+  if (n_fluid > 0 && (!pos3 || !(mass > 0))) return "fluid positions and a positive mass are required";
+  out.desc = d;
+  out.prm = p;
+  out.lat = lattice_of(d);
+  out.n_fluid = n_fluid;
+  const float w_slot = d.max_fluid > 0 ? (float)(1 / d.fluid_mass) : 0.f;
+  const float w_placed = n_fluid > 0 ? (float)(1 / mass) : 0.f;
+  out.fluid_pos.assign(d.max_fluid, make_float4(0.f, 0.f, 0.f, w_slot));
+  out.fluid_prev.assign(d.max_fluid, make_float4(0.f, 0.f, 0.f, w_slot));
+  for (int k = 0; k < n_fluid; k++) {
+    const float x = pos3[3 * k], y = pos3[3 * k + 1], z = pos3[3 * k + 2];
+    out.fluid_pos[k] = make_float4(x, y, z, w_placed);
+    out.fluid_prev[k] = make_float4(x, y, z, 0.f);
+  }
+  out.fluid_vel.clear();
+  if (vel3 && n_fluid > 0) {
+    out.fluid_vel.resize(n_fluid);
+    for (int k = 0; k < n_fluid; k++)
+      out.fluid_vel[k] = make_float4(vel3[3 * k], vel3[3 * k + 1], vel3[3 * k + 2], 0.f);
+  }
+  return nullptr;
+}
+
+cudaError_t upload_prepared(const PreparedScene& ps, const SimView& v, cudaStream_t st) {
+  const HostScene& L = *ps.lat;
+  const int S = v.S;
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+  };
+  cudaError_t e = up((void*)v.adj, L.adj.data(), L.adj.size() * 4);
+  if (e == cudaSuccess) e = up((void*)v.adj_other, L.adj_other.data(), L.adj_other.size() * 4);
+  if (e == cudaSuccess) e = up((void*)v.adj_scale, L.adj_scale.data(), L.adj_scale.size() * 4);
+  if (e == cudaSuccess) e = up((void*)v.tet_adj, L.tet_adj.data(), L.tet_adj.size() * 4);
+  if (e == cudaSuccess) e = up(v.tet_idx, L.tet_idx.data(), L.tet_idx.size() * 4);
+  if (e == cudaSuccess) e = up(v.cons, L.cons.data(), L.cons.size() * 16);
+  if (e == cudaSuccess) e = up(v.tet_vol, L.tet_vol.data(), L.tet_vol.size() * 4);
+  if (e == cudaSuccess) e = up(v.pos, L.pos.data(), (size_t)S * 16);
+  if (e == cudaSuccess) e = up(v.prev, L.pos.data(), (size_t)S * 16);
+  if (e == cudaSuccess) e = up(v.pos + S, ps.fluid_pos.data(), ps.fluid_pos.size() * 16);
+  if (e == cudaSuccess) e = up(v.prev + S, ps.fluid_prev.data(), ps.fluid_prev.size() * 16);
+  if (e == cudaSuccess) e = up(v.vel + S, ps.fluid_vel.data(), ps.fluid_vel.size() * 16);
+  if (e == cudaSuccess && S + ps.n_fluid > 0) {
+    // solids and placed fluid active (a pageable copy: staged before return)
+    std::vector<uint32_t> f((size_t)S + ps.n_fluid, F_ACTIVE);
+    e = up(v.flags, f.data(), f.size() * 4);
   }
   return e;
 }

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <memory>
 #include <vector>
 
 #include "../../include/upbd.h"
@@ -37,9 +38,10 @@ struct SceneLayout {
   size_t bytes;
 };
 
-// Fills the sizes of v from the descriptor and host scene and returns the
-// arena layout; bind_scene then points v's arrays (and *params, the scene's
-// uniform block) into an arena that starts at base.
+// Fills the sizes of v from the descriptor and host scene (full or
+// lattice-only: N = S + d.max_fluid) and returns the arena layout;
+// bind_scene then points v's arrays (and *params, the scene's uniform block)
+// into an arena that starts at base.
 SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView& v);
 void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params);
 
@@ -48,6 +50,33 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
 // 283-292): pos and prev from the host scene (fluid slots inactive with
 // their inverse mass), solids active, constraints and tets pristine.
 cudaError_t upload_scene(const HostScene& hs, const SimView& v, cudaStream_t st);
+
+// The lattice part of a scene: build_scene of the descriptor with no fluid
+// slots (N = S). Scenes whose bodies agree (dims, spacing, solid mass,
+// centres) share one entry; the cache is thread-safe and bounded.
+std::shared_ptr<const HostScene> lattice_of(const upbd_scene_desc& d);
+
+// Host data of one scene ready for upload into a fresh arena: the shared
+// lattice plus its own fluid slots, laid out as upbd_create followed by
+// upbd_emit_particles leaves them (placed slots: pos (x, y, z, 1/mass),
+// prev (x, y, z, 0), active; the other slots: (0, 0, 0, 1/fluid_mass)).
+struct PreparedScene {
+  upbd_scene_desc desc{};
+  upbd_params prm{};
+  std::shared_ptr<const HostScene> lat;
+  std::vector<float4> fluid_pos;   // max_fluid slots
+  std::vector<float4> fluid_prev;  // max_fluid slots
+  std::vector<float4> fluid_vel;   // n_fluid slots, empty = at rest
+  int n_fluid = 0;
+};
+
+// nullptr on success, else the reason (then `out` is unspecified).
+const char* prepare_scene(const upbd_scene_desc& d, const upbd_params& p, int n_fluid, const float* pos3,
+                          const float* vel3, double mass, PreparedScene& out);
+// Enqueues the uploads of a prepared scene into a zeroed arena bound to v.
+// The copies are from pageable memory: keep `ps` alive until the stream
+// has passed them.
+cudaError_t upload_prepared(const PreparedScene& ps, const SimView& v, cudaStream_t st);
 
 // nullptr when the descriptor and parameters are valid, else the reason.
 const char* check_desc(const upbd_scene_desc* d, const upbd_params* p);
