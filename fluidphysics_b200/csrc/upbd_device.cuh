@@ -230,6 +230,65 @@ __device__ __forceinline__ void lane_slots(const SimView& v, const CellHash& ch,
   }
 }
 
+// Walk the candidates of the 27 neighbour buckets as ONE sequence: cells in
+// the reference's order k = (dx+1)*9 + (dy+1)*3 + (dz+1), each bucket's PART
+// entries in bucket order (PART 0: its fluid entries, PART 1: its solids);
+// lane l of the GL group takes candidates c = l, l+GL, l+2GL, ... so the
+// lanes' shares differ by at most one. fn(e) sees each slot e. The bucket
+// ranges are looked up by their round-robin lanes (cell k by lane k mod GL),
+// scanned into sequence offsets by shuffles, and handed over in shared
+// memory. Every lane of the warp must call it; a group with `walk` false has
+// an empty sequence. At most 256 threads per block.
+template <int PART, class Fn>
+__device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Fn&& fn) {
+  __shared__ uint32_t s_base[256 / GL][28];  // slot of candidate 0 of cell k, minus its offset
+  __shared__ uint32_t s_off[256 / GL][28];   // sequence offset of cell k (s_off[.][27] = total)
+  const unsigned FULL = 0xffffffffu;
+  const uint32_t mask = (uint32_t)v.T - 1u;
+  const int g = threadIdx.x / GL;
+  uint32_t run = 0;
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const int k = lane + GL * m;
+    uint32_t s = 0, n = 0;
+    if (walk && k < 27) {
+      const uint32_t hb = ch.bucket_k(k, mask);
+      const uint32_t f = __ldg(&v.fend[hb]);
+      if (PART == 0) {
+        s = __ldg(&v.start[hb]);
+        n = f - s;
+      } else {
+        s = f;
+        n = __ldg(&v.start[hb + 1]) - f;
+      }
+    }
+    uint32_t x = n;  // inclusive scan over the group's lanes (cell order within the round)
+#pragma unroll
+    for (int d = 1; d < GL; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, x, d, GL);
+      if (lane >= d) x += y;
+    }
+    const uint32_t off = run + x - n;
+    run += __shfl_sync(FULL, x, GL - 1, GL);
+    if (k < 27) {
+      s_base[g][k] = s - off;
+      s_off[g][k] = off;
+    }
+  }
+  if (lane == 0) s_off[g][27] = run;
+  __syncwarp();
+  uint32_t k = 0, next = s_off[g][1], base = s_base[g][0];
+  for (uint32_t c = (uint32_t)lane; c < run; c += GL) {
+    while (c >= next) {  // next non-empty cell (the total ends the sequence)
+      k++;
+      next = s_off[g][k + 1];
+      base = s_base[g][k];
+    }
+    fn(base + c);
+  }
+  __syncwarp();  // the next call may rewrite this group's cells
+}
+
 __device__ __forceinline__ uint32_t cell_of(float px, float py, float pz, double inv, uint32_t mask) {
   const double cx = floor(__dmul_rn((double)px, inv));
   const double cy = floor(__dmul_rn((double)py, inv));

@@ -201,27 +201,25 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  if (act) {
-    const float H = P->fluid_h, H2 = H * H;
-    const float4* __restrict__ spos = v.spos;
-    const uint32_t NG = (uint32_t)v.N * GL;
-    const uint32_t g = myslot * GL + lane;
-    uint32_t* __restrict__ nbr = v.nbr + g;
-    uint32_t cnt = 0;
-    lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-      const float4 pj = spos[e];
-      if (e == myslot) return;
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      if (d2 >= H2) return;
-      const float q = 1.0f - sqrtf(d2) / H;
-      rho = rho + q * q;
-      rhoNear = rhoNear + q * q * q;
-      if (cnt < NL) nbr[cnt * NG] = e;  // for fluidDisp, same positions
-      cnt++;
-    });
-    v.ncount[g] = cnt;
-  }
+  const float H = P->fluid_h, H2 = H * H;
+  const float4* __restrict__ spos = v.spos;
+  const uint32_t NG = (uint32_t)v.N * GL;
+  const uint32_t g = myslot * GL + lane;
+  uint32_t* __restrict__ nbr = v.nbr + g;
+  uint32_t cnt = 0;
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) {
+    const float4 pj = spos[e];
+    if (e == myslot) return;
+    const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+    if (d2 >= H2) return;
+    const float q = 1.0f - sqrtf(d2) / H;
+    rho = rho + q * q;
+    rhoNear = rhoNear + q * q * q;
+    if (cnt < NL) nbr[cnt * NG] = e;  // for fluidDisp, same positions
+    cnt++;
+  });
+  if (act) v.ncount[g] = cnt;
   rho = lane_sum(rho);
   rhoNear = lane_sum(rhoNear);
   if (act && lane == 0) {
@@ -244,41 +242,42 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
   const uint32_t NG = (uint32_t)v.N * GL;
   const uint32_t g = myslot * GL + lane;
   const uint32_t cnt = act ? v.ncount[g] : 0u;
-  CellHash ch;
-  if (__any_sync(0xffffffffu, cnt > NL)) group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  if (act) {
-    const float maxPair = 0.05f * H;
-    const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
-    const float2 di = v.sdens[myslot];
-    const float Pi = k * (di.x - rho0);
-    const float PNi = kn * di.y;
-    const float4* __restrict__ spos = v.spos;
-    const float2* __restrict__ sdens = v.sdens;
-    auto pair = [&](uint32_t e) {
-      const float4 pj = spos[e];
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      if (d2 >= H2 || d2 < 1e-12f) return;
-      const float d = sqrtf(d2);
-      const float q = 1.0f - d / H;
-      const float2 dj = sdens[e];
-      const float Pj = k * (dj.x - rho0);
-      const float PNj = kn * dj.y;
-      float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
-      D = clampf(D, -maxPair, maxPair);
-      const float f = D / d;
-      sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
-    };
-    // the density pass listed this lane's in-range neighbours at these same
-    // positions and in walk order; a lane whose list overflowed walks again
-    if (cnt <= NL) {
-      const uint32_t* __restrict__ nbr = v.nbr + g;
-      for (uint32_t c = 0; c < cnt; c++) pair(__ldg(&nbr[c * NG]));
-    } else {
-      lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-        if (e != myslot) pair(e);
-      });
-    }
+  const float maxPair = 0.05f * H;
+  const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
+  const float2 di = act ? v.sdens[myslot] : make_float2(0.f, 0.f);
+  const float Pi = k * (di.x - rho0);
+  const float PNi = kn * di.y;
+  const float4* __restrict__ spos = v.spos;
+  const float2* __restrict__ sdens = v.sdens;
+  auto pair = [&](uint32_t e) {
+    const float4 pj = spos[e];
+    const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+    if (d2 >= H2 || d2 < 1e-12f) return;
+    const float d = sqrtf(d2);
+    const float q = 1.0f - d / H;
+    const float2 dj = sdens[e];
+    const float Pj = k * (dj.x - rho0);
+    const float PNj = kn * dj.y;
+    float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
+    D = clampf(D, -maxPair, maxPair);
+    const float f = D / d;
+    sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
+  };
+  // the density pass listed this lane's in-range neighbours at these same
+  // positions and in walk order; a lane whose list overflowed walks its
+  // share again (the whole warp takes part in the walk's shuffles)
+  const bool over = act && cnt > NL;
+  if (act && !over) {
+    const uint32_t* __restrict__ nbr = v.nbr + g;
+    for (uint32_t c = 0; c < cnt; c++) pair(__ldg(&nbr[c * NG]));
+  }
+  if (__any_sync(0xffffffffu, over)) {
+    CellHash ch;
+    group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
+    lane_strided<0>(v, ch, lane, act, [&](uint32_t e) {
+      if (over && e != myslot) pair(e);
+    });
   }
   sx = lane_sum(sx);
   sy = lane_sum(sy);
@@ -661,31 +660,30 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   const float4 pi = walk ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  if (walk) {
-    const float wi = pi.w;
-    const float rs = P->solid_radius, rf = P->fluid_radius, scale = P->contact_scale;
-    // a solid meets the fluid part of each bucket, a fluid particle the solid
-    // part (fluid-fluid is DDR's job, solid-solid the contact cache's)
-    const float ri = iSolid ? rs : rf;
-    const float rsum = ri + (iSolid ? rf : rs);
-    const float4* __restrict__ spos = v.spos;
-    auto pair = [&](uint32_t e) {
-      const float4 pj = spos[e];
-      const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      if (d2 >= rsum * rsum || d2 < 1e-12f) return;
-      const float wsum = wi + pj.w;
-      if (wsum == 0.f) return;
-      const float d = sqrtf(d2);
-      const float f = (rsum - d) / d * wi / wsum * scale;
-      cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
-      cnt = cnt + 1.0f;
-    };
-    if (iSolid)
-      lane_slots<0>(v, ch, lane, pair);
-    else
-      lane_slots<1>(v, ch, lane, pair);
-  }
+  const float wi = pi.w;
+  const float rs = P->solid_radius, rf = P->fluid_radius, scale = P->contact_scale;
+  // a solid meets the fluid part of each bucket, a fluid particle the solid
+  // part (fluid-fluid is DDR's job, solid-solid the contact cache's)
+  const float ri = iSolid ? rs : rf;
+  const float rsum = ri + (iSolid ? rf : rs);
+  const float4* __restrict__ spos = v.spos;
+  auto pair = [&](uint32_t e) {
+    const float4 pj = spos[e];
+    const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
+    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+    if (d2 >= rsum * rsum || d2 < 1e-12f) return;
+    const float wsum = wi + pj.w;
+    if (wsum == 0.f) return;
+    const float d = sqrtf(d2);
+    const float f = (rsum - d) / d * wi / wsum * scale;
+    cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
+    cnt = cnt + 1.0f;
+  };
+  // a warp holds solids or fluid or both (at the S boundary): the two walks
+  // are separate calls, each with every lane of the warp
+  const unsigned FULL = 0xffffffffu;
+  if (__any_sync(FULL, walk && iSolid)) lane_strided<0>(v, ch, lane, walk && iSolid, pair);
+  if (__any_sync(FULL, walk && !iSolid)) lane_strided<1>(v, ch, lane, walk && !iSolid, pair);
   cx = lane_sum(cx);
   cy = lane_sum(cy);
   cz = lane_sum(cz);
@@ -849,20 +847,18 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  if (act) {
-    const float H = P->fluid_h, H2 = H * H;
-    const float4* __restrict__ spos = v.spos;
-    const float4* __restrict__ svel = v.svel;
-    lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-      const float4 pj = spos[e];
-      if (e == myslot) return;
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
-      const float4 vj = svel[e];
-      sx = sx + vj.x; sy = sy + vj.y; sz = sz + vj.z;
-      m = m + 1.0f;
-    });
-  }
+  const float H = P->fluid_h, H2 = H * H;
+  const float4* __restrict__ spos = v.spos;
+  const float4* __restrict__ svel = v.svel;
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) {
+    const float4 pj = spos[e];
+    if (e == myslot) return;
+    const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+    if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
+    const float4 vj = svel[e];
+    sx = sx + vj.x; sy = sy + vj.y; sz = sz + vj.z;
+    m = m + 1.0f;
+  });
   sx = lane_sum(sx);
   sy = lane_sum(sy);
   sz = lane_sum(sz);

@@ -31,20 +31,27 @@ static constexpr uint32_t C_K = 40u;  // src/gpu/wgsl.js:25
 // Summation order of the neighbour gathers (fluidDensity, fluidDisp, xsph,
 // contacts). The reference sums one particle's neighbours in any order its
 // invocation takes; this restatement fixes the order the CUDA kernels use, so
-// the two agree bit for bit: the 27 neighbour cells k = (dx+1)*9 + (dy+1)*3 +
-// (dz+1) are dealt to GL = 8 lanes (lane l walks k = l, l+8, l+16, l+24, each
-// bucket's entries in order), every lane sums from zero, and the eight
-// partials combine as ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
+// the two agree bit for bit. The candidates of one part (fluid entries, or
+// solid entries) of the 27 neighbour buckets, cells k = (dx+1)*9 + (dy+1)*3 +
+// (dz+1) in order and each bucket's entries in order, form one sequence c =
+// 0, 1, ...; candidate c goes to lane c mod GL (GL = 8), every lane sums from
+// zero, and the eight partials combine as ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
 static constexpr int GL = 8;
 template <class R> static inline R lane_reduce(const R* p) {
   return ((p[0] + p[4]) + (p[2] + p[6])) + ((p[1] + p[5]) + (p[3] + p[7]));
 }
-template <class Sim, class V, class Fn> static inline void lane_walk(const Sim& s, const V& pi, Fn&& fn) {
-  for (int l = 0; l < GL; l++)
-    for (int k = l; k < 27; k += GL) {
-      const uint32_t h = s.cellHashOf(pi, k / 9 - 1, (k / 3) % 3 - 1, k % 3 - 1);
-      for (uint32_t e = s.start[h]; e < s.start[h + 1]; e++) fn(l, s.entries[e]);
+template <class Sim, class V, class Fn>
+static inline void strided_walk(const Sim& s, const V& pi, bool solid_part, Fn&& fn) {
+  uint32_t c = 0;
+  for (int k = 0; k < 27; k++) {
+    const uint32_t h = s.cellHashOf(pi, k / 9 - 1, (k / 3) % 3 - 1, k % 3 - 1);
+    for (uint32_t e = s.start[h]; e < s.start[h + 1]; e++) {
+      const uint32_t j = s.entries[e];
+      if ((j < (uint32_t)s.S) != solid_part) continue;
+      fn((int)(c % GL), j);
+      c++;
     }
+  }
 }
 
 template <class R> int O2Sim<R>::create(const upbd_scene_desc& d, const upbd_params& p) {
@@ -345,7 +352,7 @@ template <class R> void O2Sim<R>::passDensity() {
     if (!(flags[i] & F_ACTIVE)) continue;
     const V4<R> pi = pos[i];
     R rho[GL] = {}, rhoNear[GL] = {};
-    lane_walk(*this, pi, [&](int l, uint32_t j) {
+    strided_walk(*this, pi, false, [&](int l, uint32_t j) {
       if (j == (uint32_t)i || j < (uint32_t)S) return;
       const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
       const R d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -369,7 +376,7 @@ template <class R> void O2Sim<R>::passDisp() {
     const R Pi = P.stiffness * (density[i].x - P.restDensity);
     const R PNi = P.nearStiffness * density[i].y;
     R px[GL] = {}, py[GL] = {}, pz[GL] = {};
-    lane_walk(*this, pi, [&](int l, uint32_t j) {
+    strided_walk(*this, pi, false, [&](int l, uint32_t j) {
       if (j == (uint32_t)i || j < (uint32_t)S) return;
       const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
       const R d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -669,7 +676,8 @@ template <class R> void O2Sim<R>::passContacts() {
     const R wi = pi.w;
     const R ri = iSolid ? P.solidRadius : P.fluidRadius;
     R cx[GL] = {}, cy[GL] = {}, cz[GL] = {}, cnt[GL] = {};
-    lane_walk(*this, pi, [&](int l, uint32_t j) {
+    // a solid walks the fluid part of each bucket, a fluid particle the solids
+    strided_walk(*this, pi, !iSolid, [&](int l, uint32_t j) {
       if (j == (uint32_t)i) return;
       const bool jSolid = j < (uint32_t)S;
       if (iSolid == jSolid) return;
@@ -794,7 +802,7 @@ template <class R> void O2Sim<R>::passXsph() {
     if (!(flags[i] & F_ACTIVE)) continue;
     const V4<R> pi = pos[i];
     R qx[GL] = {}, qy[GL] = {}, qz[GL] = {}, qm[GL] = {};
-    lane_walk(*this, pi, [&](int l, uint32_t j) {
+    strided_walk(*this, pi, false, [&](int l, uint32_t j) {
       if (j == (uint32_t)i || j < (uint32_t)S) return;
       const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
       if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
