@@ -166,6 +166,8 @@ _SIGS = [
     ("upbd_rebuild_grid", C.c_int, [_P]),
     ("upbd_substep_partial", C.c_int, [_P, C.c_double, C.c_int32]),
     ("upbd_read_tets", C.c_int, [_P, _U]),
+    ("upbd_write_tets", C.c_int, [_P, _U]),
+    ("upbd_set_fluid_next", C.c_int, [_P, C.c_int32]),
     ("upbd_groups", C.c_int, [_P, C.POINTER(C.c_int32)]),
     ("upbd_grid_build", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
     ("upbd_grid_build_noalloc", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),

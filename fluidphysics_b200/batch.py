@@ -170,11 +170,21 @@ def fluid_block(n: int, r: float, y0: float, seed: int) -> np.ndarray:
     return S.jittered_block(nx, ny, nx, 2.2 * r, y0, seed)[:n]
 
 
+def compact_table(n: int) -> int:
+    """A hash table of the next power of two >= 2n buckets (at least 4,096):
+    deriveOpts's sizing rule without its 2^18 floor (src/gpu/main.js:30-54),
+    which only the reference's 256-wide scan passes needed."""
+    return max(4096, 1 << math.ceil(math.log2(max(2 * n, 2))))
+
+
 def batch_scene(dim: int, n_fluid: int, seed: int, radius_mm: float = 30, iters: int = 3,
-                gravity: float = -9.8) -> S.Scene:
+                gravity: float = -9.8, table: str = "reference") -> S.Scene:
     """One scene of the uneven batch: deriveOpts(dim, n_fluid, radius_mm) with
-    the fluid block above the body."""
+    the fluid block above the body. table "compact" sizes the hash table by
+    compact_table instead of deriveOpts's rule."""
     d, p, opts = S.gpu_scene(dim, n_fluid, radius_mm, gravity=gravity, iters=iters)
+    if table == "compact":
+        d.table_size = compact_table(dim ** 3 + n_fluid)
     r = radius_mm / 1000
     top = opts["cubeCenter"][1] + (dim - 1) * opts["spacing"] / 2
     fp = fluid_block(n_fluid, r, max(1.7, top + 3 * r), seed)
@@ -183,7 +193,7 @@ def batch_scene(dim: int, n_fluid: int, seed: int, radius_mm: float = 30, iters:
 
 
 def batch_scenes(n: int = 256, seed0: int = 1000, iters: int = 3, dims=(6, 20),
-                 fluid_log2=(11.0, 16.0)) -> list[S.Scene]:
+                 fluid_log2=(11.0, 16.0), table: str = "reference") -> list[S.Scene]:
     """The uneven batch: scene k draws its body dim uniformly from dims and
     its fluid count as floor(2^U(fluid_log2)) from numpy PCG64(seed0 + k)."""
     out = []
@@ -191,7 +201,7 @@ def batch_scenes(n: int = 256, seed0: int = 1000, iters: int = 3, dims=(6, 20),
         rng = np.random.default_rng(seed0 + k)
         dim = int(rng.integers(dims[0], dims[1] + 1))
         nf = int(math.floor(2.0 ** rng.uniform(*fluid_log2)))
-        out.append(batch_scene(dim, nf, seed0 + k, iters=iters))
+        out.append(batch_scene(dim, nf, seed0 + k, iters=iters, table=table))
     return out
 
 

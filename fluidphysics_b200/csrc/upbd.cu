@@ -960,6 +960,33 @@ int upbd_read_tets(upbd_sim* s, uint32_t* tets5) {
   return UPBD_OK;
 }
 
+int upbd_write_tets(upbd_sim* s, const uint32_t* tets5) {
+  if (!s || !tets5) return UPBD_ERR_INVALID;
+  cudaSetDevice(s->device);
+  const int NT = s->v.NT;
+  if (NT == 0) return UPBD_OK;
+  std::vector<uint32_t> idx(4 * (size_t)NT);
+  std::vector<float> vol(NT);
+  UPBD_CK(s, cudaMemcpyAsync(idx.data(), s->v.tet_idx, idx.size() * 4, cudaMemcpyDeviceToHost, s->stream));
+  UPBD_CK(s, cudaStreamSynchronize(s->stream));
+  for (int t = 0; t < NT; t++) {
+    for (int q = 0; q < 4; q++)
+      if (tets5[5 * t + q] != idx[4 * t + q]) return fail(s, UPBD_ERR_INVALID, "tet vertices must match the scene's");
+    std::memcpy(&vol[t], &tets5[5 * t + 4], 4);
+  }
+  UPBD_CK(s, cudaMemcpyAsync(s->v.tet_vol, vol.data(), vol.size() * 4, cudaMemcpyHostToDevice, s->stream));
+  UPBD_CK(s, cudaStreamSynchronize(s->stream));
+  return UPBD_OK;
+}
+
+int upbd_set_fluid_next(upbd_sim* s, int32_t next) {
+  if (!s) return UPBD_ERR_INVALID;
+  if (next < 0 || (s->v.F > 0 && next >= s->v.F) || (s->v.F == 0 && next != 0))
+    return fail(s, UPBD_ERR_INVALID, "fluid_next out of range [0, max_fluid)");
+  s->fluid_next = next;
+  return UPBD_OK;
+}
+
 // Solver._recomputeGroups, src/solver.js:488-499 — union-find with path
 // halving over alive constraints in constraint order, on the host over the
 // downloaded alive flags (the same sequential algorithm, so root ids match).

@@ -234,15 +234,20 @@ __device__ __forceinline__ void lane_slots(const SimView& v, const CellHash& ch,
 // the reference's order k = (dx+1)*9 + (dy+1)*3 + (dz+1), each bucket's PART
 // entries in bucket order (PART 0: its fluid entries, PART 1: its solids);
 // lane l of the GL group takes candidates c = l, l+GL, l+2GL, ... so the
-// lanes' shares differ by at most one. fn(e) sees each slot e. The bucket
-// ranges are looked up by their round-robin lanes (cell k by lane k mod GL),
-// scanned into sequence offsets by shuffles, and handed over in shared
-// memory. Every lane of the warp must call it; a group with `walk` false has
-// an empty sequence. At most 256 threads per block.
-template <int PART, class Fn>
-__device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Fn&& fn) {
-  __shared__ uint32_t s_base[256 / GL][28];  // slot of candidate 0 of cell k, minus its offset
-  __shared__ uint32_t s_off[256 / GL][28];   // sequence offset of cell k (s_off[.][27] = total)
+// lanes' shares differ by at most one. For each slot e of its share, in
+// order, a lane calls use(e, load(e)). The bucket ranges are looked up by
+// their round-robin lanes (cell k by lane k mod GL), scanned into sequence
+// offsets by shuffles, and handed over in shared memory. Every lane of the
+// warp must call it; a group with `walk` false has an empty sequence. At most
+// 256 threads per block.
+static __shared__ uint32_t s_walk_base[256 / GL][28];  // slot of candidate 0 of cell k, minus its offset
+static __shared__ uint32_t s_walk_off[256 / GL][28];   // sequence offset of cell k ([27] = total)
+
+template <int PART, class Load, class Use>
+__device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Load&& load,
+                                             Use&& use) {
+  auto& s_base = s_walk_base;  // shared by both parts' instantiations
+  auto& s_off = s_walk_off;
   const unsigned FULL = 0xffffffffu;
   const uint32_t mask = (uint32_t)v.T - 1u;
   const int g = threadIdx.x / GL;
@@ -278,13 +283,16 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
   if (lane == 0) s_off[g][27] = run;
   __syncwarp();
   uint32_t k = 0, next = s_off[g][1], base = s_base[g][0];
+  // one candidate per step: unrolling to keep several loads in flight cost
+  // more in registers (occupancy) than it won in latency on B200
   for (uint32_t c = (uint32_t)lane; c < run; c += GL) {
     while (c >= next) {  // next non-empty cell (the total ends the sequence)
       k++;
       next = s_off[g][k + 1];
       base = s_base[g][k];
     }
-    fn(base + c);
+    const uint32_t e = base + c;
+    use(e, load(e));
   }
   __syncwarp();  // the next call may rewrite this group's cells
 }

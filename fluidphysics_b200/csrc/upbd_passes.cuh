@@ -207,8 +207,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   const uint32_t g = myslot * GL + lane;
   uint32_t* __restrict__ nbr = v.nbr + g;
   uint32_t cnt = 0;
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) {
-    const float4 pj = spos[e];
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
     if (e == myslot) return;
     const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -249,14 +248,12 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
   const float PNi = kn * di.y;
   const float4* __restrict__ spos = v.spos;
   const float2* __restrict__ sdens = v.sdens;
-  auto pair = [&](uint32_t e) {
-    const float4 pj = spos[e];
+  auto pair = [&](const float4& pj, const float2& dj) {
     const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
     if (d2 >= H2 || d2 < 1e-12f) return;
     const float d = sqrtf(d2);
     const float q = 1.0f - d / H;
-    const float2 dj = sdens[e];
     const float Pj = k * (dj.x - rho0);
     const float PNj = kn * dj.y;
     float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
@@ -270,13 +267,16 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
   const bool over = act && cnt > NL;
   if (act && !over) {
     const uint32_t* __restrict__ nbr = v.nbr + g;
-    for (uint32_t c = 0; c < cnt; c++) pair(__ldg(&nbr[c * NG]));
+    for (uint32_t c = 0; c < cnt; c++) {
+      const uint32_t e = __ldg(&nbr[c * NG]);
+      pair(spos[e], sdens[e]);
+    }
   }
   if (__any_sync(0xffffffffu, over)) {
     CellHash ch;
     group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-    lane_strided<0>(v, ch, lane, act, [&](uint32_t e) {
-      if (over && e != myslot) pair(e);
+    lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
+      if (over && e != myslot) pair(pj, sdens[e]);
     });
   }
   sx = lane_sum(sx);
@@ -667,8 +667,8 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   const float ri = iSolid ? rs : rf;
   const float rsum = ri + (iSolid ? rf : rs);
   const float4* __restrict__ spos = v.spos;
-  auto pair = [&](uint32_t e) {
-    const float4 pj = spos[e];
+  auto load = [&](uint32_t e) { return spos[e]; };
+  auto pair = [&](uint32_t, const float4& pj) {
     const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
     if (d2 >= rsum * rsum || d2 < 1e-12f) return;
@@ -682,8 +682,8 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   // a warp holds solids or fluid or both (at the S boundary): the two walks
   // are separate calls, each with every lane of the warp
   const unsigned FULL = 0xffffffffu;
-  if (__any_sync(FULL, walk && iSolid)) lane_strided<0>(v, ch, lane, walk && iSolid, pair);
-  if (__any_sync(FULL, walk && !iSolid)) lane_strided<1>(v, ch, lane, walk && !iSolid, pair);
+  if (__any_sync(FULL, walk && iSolid)) lane_strided<0>(v, ch, lane, walk && iSolid, load, pair);
+  if (__any_sync(FULL, walk && !iSolid)) lane_strided<1>(v, ch, lane, walk && !iSolid, load, pair);
   cx = lane_sum(cx);
   cy = lane_sum(cy);
   cz = lane_sum(cz);
@@ -850,8 +850,7 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   const float H = P->fluid_h, H2 = H * H;
   const float4* __restrict__ spos = v.spos;
   const float4* __restrict__ svel = v.svel;
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) {
-    const float4 pj = spos[e];
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
     if (e == myslot) return;
     const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
     if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;

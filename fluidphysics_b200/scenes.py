@@ -69,6 +69,24 @@ PARAM_NAMES = {
 }
 
 
+# GpuSim DEFAULTS, src/gpu/sim.js:20-63, in the reference's own keys (the
+# schema of a snapshot's `opts`)
+GPU_DEFAULTS = {
+    "SOLID_DIM": 20, "SOLID_DIM2": None, "MAX_FLUID": 65536, "TABLE": 1 << 18,
+    "spacing": 0.065, "solidMass": 0.004, "fluidMass": 0.0015, "cubeCenter": [0, 1.8, 0],
+    "substeps": 5, "solidIters": 8,
+    "params": {
+        "h": 1 / 300, "gravity": -10, "solidRadius": 0.034, "fluidRadius": 0.05, "cellSize": 0.13,
+        "fluidH": 0.13, "restDensity": 3.0, "stiffness": 0.0015, "nearStiffness": 0.006,
+        "viscosity": 0.3, "compliance": 5e-4, "omega": 1.5, "plasticThreshold": 0.38,
+        "plasticRate": 0.04, "tearGap": 1.3, "maxSpeed": 14, "wallX": 3.5, "wallZ": 3.5,
+        "wallH": 0.92, "wallT": 0.07, "cullR": 7.0, "dampSolid": 1.2, "dampFluid": 0.6,
+        "frictionSolid": 0.4, "frictionFluid": 0.04, "grabK": 0.6, "sleepSpeed": 0,
+        "solidViscosity": 0,
+    },
+}
+
+
 def default_desc() -> L.SceneDesc:
     d = L.SceneDesc()
     _fill_default_desc(d)

@@ -213,6 +213,13 @@ class Sim:
             self._ck(self.lib.upbd_read_tets(self.h, L.uptr(t)))
         return t
 
+    def write_tets(self, tets5: np.ndarray) -> None:
+        t = np.ascontiguousarray(tets5, dtype=np.uint32)
+        self._ck(self.lib.upbd_write_tets(self.h, L.uptr(t)))
+
+    def set_fluid_next(self, k: int) -> None:
+        self._ck(self.lib.upbd_set_fluid_next(self.h, int(k)))
+
     def groups(self) -> np.ndarray:
         g = np.empty(self.info.solid_n, np.int32)
         self._ck(self.lib.upbd_groups(self.h, g.ctypes.data_as(C.POINTER(C.c_int32))))
@@ -242,6 +249,12 @@ class GpuSim:
         self.params = S.default_params()
         S.set_params(self.params, opts.get("params", {}))
         self.sim = Sim(self.desc, self.params, variant)
+        # the merged options of the constructor (src/gpu/sim.js:78-84), with
+        # the companion cube's size resolved: what a snapshot carries
+        o = {**S.GPU_DEFAULTS, **{k: v for k, v in opts.items() if k != "params"}}
+        o["params"] = {**S.GPU_DEFAULTS["params"], **opts.get("params", {})}
+        o["SOLID_DIM2"] = int(self.desc.solid_dim2)
+        self.o = o
         i = self.sim.info
         self.SOLID_N, self.N1, self.TOTAL = i.solid_n, i.n1, i.total
         self.DIM2, self.NUM_CONS, self.NUM_TETS = i.dim2, i.num_cons, i.num_tets

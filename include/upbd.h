@@ -286,6 +286,13 @@ int upbd_rebuild_grid(upbd_sim* sim);
 int upbd_substep_partial(upbd_sim* sim, double h, int32_t last_pass);
 /* Tets: tets5[num_tets*5] = {a, b, c, d, rest volume bits (negative = dead)}. */
 int upbd_read_tets(upbd_sim* sim, uint32_t* tets5);
+/* The tet part of GpuSim.restore (src/gpu/sim.js:528-535): writes the rest
+ * volumes (sign = alive) of tets5 back; the vertex indices must be the
+ * scene's own. */
+int upbd_write_tets(upbd_sim* sim, const uint32_t* tets5);
+/* GpuSim.restore's fluidNext (src/gpu/sim.js:544): the next emit slot of the
+ * hose ring buffer, 0 <= next < max_fluid. */
+int upbd_set_fluid_next(upbd_sim* sim, int32_t next);
 /* Solver._recomputeGroups — src/solver.js:488-499: union-find over alive
  * constraints; group[solid_n] = root id. */
 int upbd_groups(upbd_sim* sim, int32_t* group);
