@@ -151,10 +151,9 @@ struct CellHash {
   }
 };
 
-// Neighbour gathers run GL lanes per particle: lane l walks the neighbour
-// cells k = l, l+GL, l+2GL, l+3GL (k < 27, in the reference's dx/dy/dz order)
-// and each bucket's entries in order, accumulating its own partial sums from
-// zero; the GL partials are then combined by a fixed xor butterfly, so the
+// Neighbour gathers run GL lanes per particle (lane_strided below deals the
+// candidates to the lanes); each lane accumulates its own partial sums from
+// zero and the GL partials are combined by a fixed xor butterfly, so the
 // result is deterministic: ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
 constexpr int GL = 8;
 constexpr uint32_t NL = 16;  // neighbour-list entries kept per lane
@@ -193,11 +192,11 @@ __device__ __forceinline__ void group_cell_hash(float px, float py, float pz, do
   ch.hz[2] = __shfl_sync(FULL, v2, base + 0);
 }
 
-// Walk this lane's neighbour cells: all bucket ranges are loaded first
-// (independent loads), then the candidates of the four buckets as one flat
-// sequence (bucket order, entries in order). PART 0 walks each bucket's fluid
-// entries, PART 1 its solid entries; fn(e) sees each slot e (the caller reads
-// the slot's bucket-ordered copies).
+// Walk this lane's share of the neighbour cells, k = lane, lane+GL, ... (for
+// passes whose result does not depend on the order, the contact marks): all
+// bucket ranges are loaded first (independent loads), then the candidates of
+// the buckets as one flat sequence. PART 0 walks each bucket's fluid entries,
+// PART 1 its solid entries; fn(e) sees each slot e.
 template <int PART, class Fn>
 __device__ __forceinline__ void lane_slots(const SimView& v, const CellHash& ch, int lane, Fn&& fn) {
   const uint32_t mask = (uint32_t)v.T - 1u;
