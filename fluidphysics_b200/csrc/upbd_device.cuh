@@ -296,6 +296,17 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
   __syncwarp();  // the next call may rewrite this group's cells
 }
 
+// Square roots inside the gathers' candidate loops. The parity build keeps
+// the correctly rounded operations of the reference's expressions (its results
+// match the oracle bit for bit); the product build uses the hardware
+// approximation (sqrt.approx.f32, exact at 0) and reciprocal square root, which
+// stay within the stated per-substep tolerance and keep the loops short.
+__device__ __forceinline__ float approx_sqrt(float x) {
+  float y;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ uint32_t cell_of(float px, float py, float pz, double inv, uint32_t mask) {
   const double cx = floor(__dmul_rn((double)px, inv));
   const double cy = floor(__dmul_rn((double)py, inv));

@@ -207,16 +207,30 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   const uint32_t g = myslot * GL + lane;
   uint32_t* __restrict__ nbr = v.nbr + g;
   uint32_t cnt = 0;
+#ifndef UPBD_PARITY_BUILD
+  const float invH = 1.0f / H;
+#endif
   lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
-    if (e == myslot) return;
     const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+#ifdef UPBD_PARITY_BUILD
+    if (e == myslot) return;
     if (d2 >= H2) return;
     const float q = 1.0f - sqrtf(d2) / H;
     rho = rho + q * q;
     rhoNear = rhoNear + q * q * q;
     if (cnt < NL) nbr[cnt * NG] = e;  // for fluidDisp, same positions
     cnt++;
+#else
+    // branch-free: every lane of the warp takes the same path per candidate
+    const bool in = (e != myslot) && (d2 < H2);
+    const float q = 1.0f - approx_sqrt(d2) * invH;
+    const float qq = in ? q * q : 0.0f;
+    rho = rho + qq;
+    rhoNear = rhoNear + qq * q;
+    if (in && cnt < NL) nbr[cnt * NG] = e;  // for fluidDisp, same positions
+    cnt += in ? 1u : 0u;
+#endif
   });
   if (act) v.ncount[g] = cnt;
   rho = lane_sum(rho);
@@ -248,17 +262,30 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
   const float PNi = kn * di.y;
   const float4* __restrict__ spos = v.spos;
   const float2* __restrict__ sdens = v.sdens;
+#ifndef UPBD_PARITY_BUILD
+  const float invH = 1.0f / H;
+#endif
   auto pair = [&](const float4& pj, const float2& dj) {
     const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
     if (d2 >= H2 || d2 < 1e-12f) return;
+#ifdef UPBD_PARITY_BUILD
     const float d = sqrtf(d2);
     const float q = 1.0f - d / H;
+#else
+    const float rd = rsqrtf(d2);  // d2 >= 1e-12 here
+    const float d = d2 * rd;
+    const float q = 1.0f - d * invH;
+#endif
     const float Pj = k * (dj.x - rho0);
     const float PNj = kn * dj.y;
     float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
     D = clampf(D, -maxPair, maxPair);
+#ifdef UPBD_PARITY_BUILD
     const float f = D / d;
+#else
+    const float f = D * rd;
+#endif
     sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
   };
   // the density pass listed this lane's in-range neighbours at these same
@@ -674,8 +701,13 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
     if (d2 >= rsum * rsum || d2 < 1e-12f) return;
     const float wsum = wi + pj.w;
     if (wsum == 0.f) return;
+#ifdef UPBD_PARITY_BUILD
     const float d = sqrtf(d2);
     const float f = (rsum - d) / d * wi / wsum * scale;
+#else
+    const float rd = rsqrtf(d2);  // d2 >= 1e-12 here
+    const float f = (rsum - d2 * rd) * rd * __fdividef(wi, wsum) * scale;
+#endif
     cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
     cnt = cnt + 1.0f;
   };
