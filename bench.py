@@ -322,6 +322,47 @@ def run_batched(args, stream, hbm: float) -> dict:
     }
 
 
+def run_large(args, stream) -> dict:
+    """The large scene: 24^3 = 13,824 body + 262,144 fluid at 30 mm, a hose of
+    120 particles per frame from a seeded nozzle and 64 grabbed body particles
+    moved on y0 + 0.3 sin(pi t), through the single-scene handle; each frame
+    timed by CUDA events. The closest scene to the reference's published
+    14k body + 253k water figure (README.md:14)."""
+    import torch
+    from fluidphysics_b200 import scenes as S
+    from fluidphysics_b200.sim import sim_from_scene
+    K = args.large_frames
+    sc = S.large(frames=K + 3)
+    sim = sim_from_scene(sc)
+    sim.set_stream(stream.cuda_stream)
+    idx = S.grab_set(sim.read_state()["pos"], sc.solid_n, sc.desc.solid_dim, sc.grab_count)
+    sim.grab_indices(idx)
+    hose = S.hose_script(sc, K + 3)
+    w = 2 * math.pi * sc.grab_freq_hz
+    evs = []
+    for k in range(K + 3):
+        pos, dr, side, up, speed, phase = hose[k]
+        sim.emit(sc.hose_per_frame, pos, dr, side, up, speed, phase)
+        sim.grab_move([0.0, sc.grab_amp * (math.sin(w * (k + 1) * sc.dt) - math.sin(w * k * sc.dt)), 0.0])
+        timed = k >= 3  # three warm-up frames capture the graphs
+        if timed:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        sim.step(sc.dt, sc.substeps)
+        if timed:
+            b.record(stream)
+            evs.append((a, b))
+    sim.sync()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    active = sc.solid_n + sim.active_count()
+    sim.close()
+    return {"value": active * sc.substeps * K / (ms / 1e3), "unit": UNIT, "ms_per_frame": ms / K, "frames": K,
+            "workload": "24^3 body (13,824) + 262,144 fluid, 30 mm, hose 120/frame, 64-particle grab on "
+                        "y0 + 0.3 sin(pi t), 5 substeps x 3 iterations",
+            "reference_published": "19 ms per frame for 14k body + 253k water on an RTX PRO 6000 under "
+                                   "WebGPU (README.md:14; other hardware, substep count unstated)"}
+
+
 def run_served(args, batched: dict | None) -> dict:
     """The served stream: Poisson arrivals at 200 scenes/s for
     --served-window seconds; each request a scene of 1k-262k particles (body
@@ -374,6 +415,8 @@ def main() -> None:
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--served-window", type=float, default=2.0,
                     help="seconds of Poisson arrivals served (0 skips the served line)")
+    ap.add_argument("--large-frames", type=int, default=120,
+                    help="timed frames of the large scene (0 skips the large line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -534,10 +577,11 @@ def main() -> None:
     roofline["step_frac"] = step_gbs / hbm
 
     sim.close()
+    large = run_large(args, stream) if args.large_frames > 0 else None
     batched = run_batched(args, stream, hbm) if args.batched_frames > 0 else None
     served = run_served(args, batched) if args.served_window > 0 else None
     if pg:
-        for key, obj in (("batched", batched), ("served", served)):
+        for key, obj in (("large", large), ("batched", batched), ("served", served)):
             if obj and obj.get("value"):
                 t = torch.tensor([obj["value"]], device="cuda", dtype=torch.float64)
                 pg.all_reduce(t, op=pg.ReduceOp.SUM)  # replicas: whole-job rate
@@ -569,6 +613,7 @@ def main() -> None:
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clk,
+            "large": large,
             "batched": batched,
             "served": served,
         }
