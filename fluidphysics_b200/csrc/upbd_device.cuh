@@ -192,43 +192,6 @@ __device__ __forceinline__ void group_cell_hash(float px, float py, float pz, do
   ch.hz[2] = __shfl_sync(FULL, v2, base + 0);
 }
 
-// Walk this lane's share of the neighbour cells, k = lane, lane+GL, ... (for
-// passes whose result does not depend on the order, the contact marks): all
-// bucket ranges are loaded first (independent loads), then the candidates of
-// the buckets as one flat sequence. PART 0 walks each bucket's fluid entries,
-// PART 1 its solid entries; fn(e) sees each slot e.
-template <int PART, class Fn>
-__device__ __forceinline__ void lane_slots(const SimView& v, const CellHash& ch, int lane, Fn&& fn) {
-  const uint32_t mask = (uint32_t)v.T - 1u;
-  uint32_t s[4], n[4];
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
-    const int k = lane + GL * m;
-    if (k < 27) {
-      const uint32_t hb = ch.bucket_k(k, mask);
-      const uint32_t f = __ldg(&v.fend[hb]);
-      if (PART == 0) {
-        s[m] = __ldg(&v.start[hb]);
-        n[m] = f - s[m];
-      } else {
-        s[m] = f;
-        n[m] = __ldg(&v.start[hb + 1]) - f;
-      }
-    } else {
-      s[m] = 0;
-      n[m] = 0;
-    }
-  }
-  const uint32_t n01 = n[0] + n[1], n012 = n01 + n[2], total = n012 + n[3];
-  for (uint32_t c = 0; c < total; c++) {
-    const uint32_t e = (c < n[0]) ? s[0] + c
-                     : (c < n01) ? s[1] + (c - n[0])
-                     : (c < n012) ? s[2] + (c - n01)
-                                  : s[3] + (c - n012);
-    fn(e);
-  }
-}
-
 // Walk the candidates of the 27 neighbour buckets as ONE sequence: cells in
 // the reference's order k = (dx+1)*9 + (dy+1)*3 + (dz+1), each bucket's PART
 // entries in bucket order (PART 0: its fluid entries, PART 1: its solids);

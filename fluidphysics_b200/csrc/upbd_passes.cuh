@@ -174,7 +174,7 @@ __device__ __forceinline__ void b_rankfix(const SimView& v, uint32_t vb) {
 }
 
 // ------------------------------------------------------------------ fluid
-// The neighbour gathers run GL lanes per particle (see lane_slots): a warp
+// The neighbour gathers run GL lanes per particle (see lane_strided): a warp
 // holds 32/GL particles, every lane reaches the shuffles, and lane 0 writes.
 // Groups take the particles in slot order (group g: the particle at slot g of
 // this substep's grid, entries[g]): the particles of one bucket sit in
@@ -401,13 +401,11 @@ __device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParam
                                                 bool act, int lane) {
   CellHash ch;
   group_cell_hash(p.x, p.y, p.z, P->inv_cell, ch);
-  if (!act) return;
   const float rsum = P->solid_radius + P->fluid_radius;
   const float lim2 = rsum * rsum * 1.00001f;
   const float4* __restrict__ spos = v.spos;
   uint32_t* __restrict__ mark = v.mark;
-  lane_slots<0>(v, ch, lane, [&](uint32_t e) {
-    const float4 pj = spos[e];
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
     const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
     if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
   });
