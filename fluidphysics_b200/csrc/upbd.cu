@@ -176,7 +176,7 @@ int launch_substep(upbd_sim* s, int last) {
   }
   PROF(s, K_INTEGRATE, k_integrate_count<true, true><<<blocks_for(v.N), 256, 0, st>>>(v, P));
   PROF(s, K_SCAN, k_scan<<<v.num_tiles, SCAN_THREADS, 0, st>>>(v));
-  PROF(s, K_SCATTER, k_scatter<<<blocks_for(std::max(v.N, v.num_tiles)), 256, 0, st>>>(v));
+  PROF(s, K_SCATTER, k_scatter<<<blocks_for(std::max(v.N, tile_words(v.num_tiles))), 256, 0, st>>>(v));
   PROF(s, K_RANKFIX, k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v));
   L += 4;
   UPBD_KCK(s);
@@ -921,7 +921,7 @@ int upbd_rebuild_grid(upbd_sim* s) {
   cudaStream_t st = s->stream;
   k_integrate_count<false, true><<<blocks_for(v.N), 256, 0, st>>>(v, s->dparams);
   k_scan<<<v.num_tiles, SCAN_THREADS, 0, st>>>(v);
-  k_scatter<<<blocks_for(std::max(v.N, v.num_tiles)), 256, 0, st>>>(v);
+  k_scatter<<<blocks_for(std::max(v.N, tile_words(v.num_tiles))), 256, 0, st>>>(v);
   k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v);
   s->launches += 4;
   UPBD_KCK(s);
@@ -1047,7 +1047,8 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
       pd.mem = nullptr;
     }
     const size_t nc = std::max<size_t>((size_t)n, pd.n_cap), tc = std::max<size_t>((size_t)table_size, pd.t_cap);
-    const size_t bytes = (tc + 3 * nc + (tc + SCAN_TILE - 1) / SCAN_TILE + 64) * 4 + sizeof(DevParams);
+    // tile_words() does not decrease with the tile count: the capacity's words cover every smaller table
+    const size_t bytes = (tc + 3 * nc + tile_words((int)((tc + SCAN_TILE - 1) / SCAN_TILE)) + 64) * 4 + sizeof(DevParams);
     if (cudaMalloc(&pd.mem, bytes) != cudaSuccess) return fail(nullptr, UPBD_ERR_OOM, "grid scratch allocation failed");
     if (cudaMemset(pd.mem, 0, bytes) != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, "grid scratch clear failed");
     pd.n_cap = nc;
@@ -1068,14 +1069,14 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
   v.start = (uint32_t*)offsets;
   v.entries = (uint32_t*)entries;
   // the count kernel reads 1/cell_size from a params block at the pool's tail
-  DevParams* dp = (DevParams*)(v.tile_sum + (pd.t_cap + SCAN_TILE - 1) / SCAN_TILE + 64);
+  DevParams* dp = (DevParams*)(v.tile_sum + tile_words((int)((pd.t_cap + SCAN_TILE - 1) / SCAN_TILE)) + 64);
   DevParams hp{};
   hp.inv_cell = 1.0 / cell_size;
   if (cudaMemcpyAsync(dp, &hp, sizeof(DevParams), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return fail(nullptr, UPBD_ERR_CUDA, "params upload failed");
   k_integrate_count<false, true><<<blocks_for(n), 256, 0, st>>>(v, dp);
   k_scan<<<tiles, SCAN_THREADS, 0, st>>>(v);
-  k_scatter<<<blocks_for(std::max(n, tiles)), 256, 0, st>>>(v);
+  k_scatter<<<blocks_for(std::max(n, tile_words(tiles))), 256, 0, st>>>(v);
   k_rankfix<<<blocks_for(n), 256, 0, st>>>(v);
   cudaError_t e = cudaPeekAtLastError();
   if (e != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, cudaGetErrorString(e));
@@ -1146,7 +1147,7 @@ constexpr size_t kNaTicket = kNaCounts + kNoAllocMaxT;
 constexpr size_t kNaCell = kNaTicket + kNoAllocMaxN;
 constexpr size_t kNaTmp = kNaCell + kNoAllocMaxN;
 constexpr size_t kNaTiles = kNaTmp + kNoAllocMaxN;
-constexpr size_t kNaParams = ((kNaTiles + kNoAllocTiles + 63) / 64) * 64;  // 256-byte aligned
+constexpr size_t kNaParams = ((kNaTiles + tile_words((int)kNoAllocTiles) + 63) / 64) * 64;  // 256-byte aligned
 constexpr size_t kNaWords = kNaParams + (sizeof(DevParams) + 3) / 4;
 
 __device__ __align__(256) uint32_t g_grid_scratch[kNaWords];
@@ -1214,12 +1215,12 @@ extern "C" int upbd_grid_build_noalloc(const void* pos4, const void* flags, int3
   // the array keeps the previous call's contents: counts and tile totals
   // must start at zero
   cudaError_t e = cudaMemsetAsync(v.counts, 0, (size_t)table_size * 4, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(v.tile_sum, 0, (size_t)tiles * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(v.tile_sum, 0, (size_t)tile_words(tiles) * 4, st);
   if (e != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, std::string("scratch clear: ") + cudaGetErrorString(e));
   k_noalloc_params<<<1, 1, 0, st>>>(dp, 1.0 / cell_size);
   k_integrate_count<false, true><<<blocks_for(n), 256, 0, st>>>(v, dp);
   k_scan<<<tiles, SCAN_THREADS, 0, st>>>(v);
-  k_scatter<<<blocks_for(std::max(n, tiles)), 256, 0, st>>>(v);
+  k_scatter<<<blocks_for(std::max(n, tile_words(tiles))), 256, 0, st>>>(v);
   k_rankfix<<<blocks_for(n), 256, 0, st>>>(v);
   if (counts) k_counts_from_offsets<<<blocks_for(table_size), 256, 0, st>>>(v.start, (uint32_t*)counts, table_size);
   e = cudaPeekAtLastError();

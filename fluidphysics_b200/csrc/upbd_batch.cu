@@ -182,7 +182,7 @@ void scene_blocks(const SimView& v, bool tets, int bt, uint32_t out[NUM_DOMAINS]
   const int nt = tets ? v.NT : 0;
   out[D_N] = ceil_div(v.N, bt);
   out[D_TILES] = (uint32_t)std::max(v.num_tiles, 1);
-  out[D_SCATTER] = ceil_div(std::max(v.N, v.num_tiles), bt);
+  out[D_SCATTER] = ceil_div(std::max(v.N, tile_words(v.num_tiles)), bt);
   out[D_FGL] = ceil_div((long long)v.N * GL, bt);
   out[D_F] = ceil_div(v.F, bt);
   out[D_SOLVE0] = ceil_div((long long)sp + v.F, bt);

@@ -24,6 +24,20 @@ constexpr uint32_t C_K = 40u;           // solid contact cache width, src/gpu/wg
 constexpr int SCAN_TILE = 2048;         // counts scanned per block
 constexpr int SCAN_THREADS = 256;       // 8 counts per thread
 
+// The count pass adds every arrival to its scan tile's total. With 2^18
+// buckets there are only 128 tiles, so one counter per tile took ~600 atomics
+// at one L2 address per substep and the kernel's drain dominated its time.
+// Each tile therefore has `tile_reps` counters, a warp adding to counter
+// (warp index mod reps): tile_sum[r * num_tiles + t]. The scan sums them back;
+// reps * num_tiles stays <= 2048 words up to 2^22 buckets, so that sum is at
+// most 8 independent loads per scan thread.
+__host__ __device__ constexpr int tile_reps(int num_tiles) {
+  int r = 16;
+  while (r > 1 && r * num_tiles > 2048) r >>= 1;
+  return r;
+}
+__host__ __device__ constexpr int tile_words(int num_tiles) { return tile_reps(num_tiles) * num_tiles; }
+
 // scratch words (device)
 constexpr int SCR_PICK_T = 0;      // uint64 bits of the best t (words 0-1)
 constexpr int SCR_PICK_I = 2;      // best index

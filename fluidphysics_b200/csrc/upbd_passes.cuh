@@ -76,65 +76,94 @@ __device__ __forceinline__ void b_integrate_count(const SimView& v, const DevPar
     const uint32_t h = cell_of(p4.x, p4.y, p4.z, P->inv_cell, (uint32_t)v.T - 1u);
     v.cell[i] = h;
     v.ticket[i] = atomicAdd(&v.counts[h], 1u);
-    atomicAdd(&v.tile_sum[h / SCAN_TILE], 1u);
+    const int rep = (i >> 5) & (tile_reps(v.num_tiles) - 1);  // a power of two
+    atomicAdd(&v.tile_sum[rep * v.num_tiles + (int)(h / SCAN_TILE)], 1u);
   }
 }
 
 // ------------------------------------------------------------ exclusive scan
 // scanBlocks/scanPartials/scanApply (src/gpu/wgsl.js:180-236) as one launch:
-// block b first sums the totals of tiles < b (kept by the count), then scans
-// its own 2048 counts, writes start[], and clears the counts it read.
+// block b scans its own 2048 counts (8 consecutive ones per thread), adds the
+// totals of tiles < b (the count's tile counters, all replicas), writes
+// start[], and clears the counts it read. The counts and the earlier totals
+// are loaded up front so that their latencies overlap, and one block barrier
+// publishes both per-warp sums.
 __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
-  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
-  __shared__ uint32_t s_base;
+  __shared__ uint32_t s_scan[SCAN_THREADS / 32];  // per-warp sums of this tile's counts
+  __shared__ uint32_t s_prev[SCAN_THREADS / 32];  // per-warp sums of earlier tiles' totals
   const int tid = threadIdx.x;
   const int lane = tid & 31, wid = tid >> 5;
-  // base = sum of totals of earlier tiles
-  uint32_t acc = 0;
-  for (int t = tid; t < (int)vb; t += SCAN_THREADS) acc += v.tile_sum[t];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if (lane == 0) s_warp[wid] = acc;
-  __syncthreads();
-  if (tid == 0) {
-    uint32_t b = 0;
-    for (int w = 0; w < SCAN_THREADS / 32; w++) b += s_warp[w];
-    s_base = b;
-  }
-  __syncthreads();
-  const uint32_t base = s_base;
-  // thread-local scan of 8 counts
   const long long t0 = (long long)vb * SCAN_TILE + (long long)tid * 8;
+  // 16-byte rows when the tile is whole and the arrays allow it (start[] may
+  // be a caller's buffer at any 4-byte offset)
+  const bool vec = t0 + 8 <= (long long)v.T && ((reinterpret_cast<uintptr_t>(v.counts) | reinterpret_cast<uintptr_t>(v.start) |
+                                                 reinterpret_cast<uintptr_t>(v.fend)) & 15u) == 0;
   uint32_t c[8];
-  uint32_t sum = 0;
+  if (vec) {
+    const uint4 a = *reinterpret_cast<const uint4*>(v.counts + t0);
+    const uint4 b = *reinterpret_cast<const uint4*>(v.counts + t0 + 4);
+    c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w;
+    c[4] = b.x; c[5] = b.y; c[6] = b.z; c[7] = b.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] = (t0 + k < (long long)v.T) ? v.counts[t0 + k] : 0u;
+  }
+  // earlier tiles: word j holds replica j / num_tiles of tile j % num_tiles
+  const int nt = v.num_tiles, words = tile_words(nt);
+  uint32_t acc = 0;
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    const long long idx = t0 + k;
-    c[k] = (idx < v.T) ? v.counts[idx] : 0u;
-    sum += c[k];
+    const int j = tid + k * SCAN_THREADS;
+    if (j < words && (uint32_t)(j % nt) < vb) acc += v.tile_sum[j];
   }
-  // block exclusive scan of thread sums
-  uint32_t x = sum;
+  for (int j = tid + 8 * SCAN_THREADS; j < words; j += SCAN_THREADS)  // past 2^22 buckets only
+    if ((uint32_t)(j % nt) < vb) acc += v.tile_sum[j];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) sum += c[k];
+  uint32_t x = sum;  // inclusive scan of the thread sums within the warp
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
   }
+  acc = __reduce_add_sync(0xffffffffu, acc);
+  if (lane == 31) s_scan[wid] = x;
+  if (lane == 0) s_prev[wid] = acc;
   __syncthreads();
-  if (lane == 31) s_warp[wid] = x;
-  __syncthreads();
-  uint32_t wbase = 0;
-  for (int w = 0; w < wid; w++) wbase += s_warp[w];
-  uint32_t run = base + wbase + x - sum;
+  uint32_t run = x - sum;
+#pragma unroll
+  for (int w = 0; w < SCAN_THREADS / 32; w++) {
+    run += s_prev[w];
+    if (w < wid) run += s_scan[w];
+  }
+  uint32_t r[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    const long long idx = t0 + k;
-    if (idx < v.T) {
-      v.start[idx] = run;
-      if (v.fend) v.fend[idx] = run;  // empty buckets; rankfix sets occupied ones
-      v.counts[idx] = 0u;  // ready for the next count
-    }
+    r[k] = run;
     run += c[k];
+  }
+  if (vec) {
+    const uint4 a = make_uint4(r[0], r[1], r[2], r[3]), b = make_uint4(r[4], r[5], r[6], r[7]);
+    *reinterpret_cast<uint4*>(v.start + t0) = a;
+    *reinterpret_cast<uint4*>(v.start + t0 + 4) = b;
+    if (v.fend) {  // empty buckets; rankfix sets occupied ones
+      *reinterpret_cast<uint4*>(v.fend + t0) = a;
+      *reinterpret_cast<uint4*>(v.fend + t0 + 4) = b;
+    }
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);  // ready for the next count
+    *reinterpret_cast<uint4*>(v.counts + t0) = z;
+    *reinterpret_cast<uint4*>(v.counts + t0 + 4) = z;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const long long idx = t0 + k;
+      if (idx < v.T) {
+        v.start[idx] = r[k];
+        if (v.fend) v.fend[idx] = r[k];
+        v.counts[idx] = 0u;
+      }
+    }
   }
   if (vb == (uint32_t)v.num_tiles - 1u && tid == SCAN_THREADS - 1) v.start[v.T] = run;
 }
@@ -143,7 +172,7 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
 // second atomic), and clear the tile totals for the next count.
 __device__ __forceinline__ void b_scatter(const SimView& v, uint32_t vb) {
   const int i = UPBD_VTID;
-  if (i < v.num_tiles) v.tile_sum[i] = 0u;
+  if (i < tile_words(v.num_tiles)) v.tile_sum[i] = 0u;
   if (i >= v.N) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
   const uint32_t h = v.cell[i];

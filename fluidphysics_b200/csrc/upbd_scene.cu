@@ -174,7 +174,7 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.tmp = cv.take<uint32_t>(v.N);
   L.ticket = cv.take<uint32_t>(v.N);
   L.cell = cv.take<uint32_t>(v.N);
-  L.tiles = cv.take<uint32_t>(v.num_tiles);
+  L.tiles = cv.take<uint32_t>(tile_words(v.num_tiles));
   L.tidx = cv.take<uint32_t>(4 * (size_t)std::max(v.NT, 1));
   L.tvol = cv.take<float>(std::max(v.NT, 1));
   L.tadj = cv.take<uint32_t>(hs.tet_adj.size());
