@@ -202,12 +202,25 @@ int launch_substep(upbd_sim* s, int last) {
   // position update of the solve; otherwise they get their own launch
   const bool mark_in_apply = iters > 0 && !tets && !scc;
   const int solid_pad = ((v.S * GL + 31) / 32) * 32;  // lane threads of the solve, whole warps
-  for (int it = 0; it < iters; it++) {
+  // with two or more plain iterations each one is a single launch that also
+  // applies (b_solid_solve's OUT); the last marks the fluid near the solids
+  const bool fold = iters >= 2 && !tets && !scc;
+  for (int it = 0; it < iters && fold; it++) {
     if (it == 0)
-      PROF(s, K_SOLID_SOLVE,
-           k_solid_solve<true><<<blocks_for((long long)solid_pad + v.F), 256, 0, st>>>(v, P, solid_pad));
+      PROF(s, K_SOLID_SOLVE, k_solid_solve<true, SOLVE_STEP>
+           <<<blocks_for((long long)solid_pad + v.F), 256, 0, st>>>(v, P, solid_pad, it));
+    else if (it < iters - 1)
+      PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_STEP><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));
     else
-      PROF(s, K_SOLID_SOLVE, k_solid_solve<false><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad));
+      PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_LAST><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));
+    L++;
+  }
+  for (int it = 0; it < iters && !fold; it++) {
+    if (it == 0)
+      PROF(s, K_SOLID_SOLVE, k_solid_solve<true, SOLVE_DELTA>
+           <<<blocks_for((long long)solid_pad + v.F), 256, 0, st>>>(v, P, solid_pad, it));
+    else
+      PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_DELTA><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));
     if (mark_in_apply && it == iters - 1)
       PROF(s, K_APPLY_SOLID, k_apply_solid<true><<<blocks_for((long long)v.S * GL), 256, 0, st>>>(v, P));
     else
@@ -253,10 +266,12 @@ int launch_substep(upbd_sim* s, int last) {
     L += 2;
   }
   if (last < UPBD_PASS_XSPH) return UPBD_OK;
-  PROF(s, K_XSPH, k_xsph<<<blocks_for((long long)v.N * GL), 256, 0, st>>>(v, P));
-  L++;
-  if (last < UPBD_PASS_XSPH_APPLY) return UPBD_OK;
-  PROF(s, K_XSPH_APPLY, k_xsph_apply<<<blocks_for(v.F), 256, 0, st>>>(v));
+  if (last < UPBD_PASS_XSPH_APPLY) {  // stop with the result in delta, as the reference's xsph pass leaves it
+    PROF(s, K_XSPH, k_xsph<false><<<blocks_for((long long)v.N * GL), 256, 0, st>>>(v, P));
+    L++;
+    return UPBD_OK;
+  }
+  PROF(s, K_XSPH, k_xsph<true><<<blocks_for((long long)v.N * GL), 256, 0, st>>>(v, P));
   L++;
   UPBD_KCK(s);
   return UPBD_OK;

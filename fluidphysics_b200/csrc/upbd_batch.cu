@@ -115,10 +115,10 @@ __global__ void __launch_bounds__(256) kb_disp(BatchArgs a) {
 __global__ void __launch_bounds__(256) kb_apply_fluid(BatchArgs a) {
   batch_loop<D_F, false>(a, UPBD_BODY { b_apply_fluid(v, vb); });
 }
-template <bool APPLY_FLUID>
-__global__ void __launch_bounds__(256) kb_solid_solve(BatchArgs a) {
+template <bool APPLY_FLUID, int OUT>
+__global__ void __launch_bounds__(256) kb_solid_solve(BatchArgs a, int it) {
   batch_loop<APPLY_FLUID ? D_SOLVE0 : D_SOLVE, false>(
-      a, UPBD_BODY { b_solid_solve<APPLY_FLUID>(v, P, solid_pad_of(v.S), vb); });
+      a, UPBD_BODY { b_solid_solve<APPLY_FLUID, OUT>(v, P, solid_pad_of(v.S), it, vb); });
 }
 template <bool MARK>
 __global__ void __launch_bounds__(256) kb_apply_solid(BatchArgs a) {
@@ -159,10 +159,7 @@ __global__ void __launch_bounds__(256) kb_solid_visc_apply(BatchArgs a) {
   });
 }
 __global__ void __launch_bounds__(256) kb_xsph(BatchArgs a) {
-  batch_loop<D_FGL, false>(a, UPBD_BODY { b_xsph(v, P, vb); });
-}
-__global__ void __launch_bounds__(256) kb_xsph_apply(BatchArgs a) {
-  batch_loop<D_F, false>(a, UPBD_BODY { b_xsph_apply(v, vb); });
+  batch_loop<D_FGL, false>(a, UPBD_BODY { b_xsph<true>(v, P, vb); });
 }
 __global__ void __launch_bounds__(256) kb_count_active(BatchArgs a) {
   batch_loop<D_F, true>(a, UPBD_BODY { b_count_active(v, vb, nblk); });
@@ -419,6 +416,7 @@ int launch_batch_frame(upbd_batch* b, int nsub, bool visc) {
   const bool scc = (b->desc.features & UPBD_FEAT_SOLID_CONTACTS) != 0;
   const int iters = b->desc.solid_iters;
   const bool mark_in_apply = iters > 0 && !tets && !scc;
+  const bool fold = iters >= 2 && !tets && !scc;  // solve + apply in one launch per iteration
   for (int k = 0; k < nsub; k++) {
     BLAUNCH(b, K_INTEGRATE, kb_integrate_count<true, true><<<G, BT, 0, st>>>(a));
     BLAUNCH(b, K_SCAN, kb_scan<<<G, SCAN_THREADS, 0, st>>>(a));
@@ -428,9 +426,14 @@ int launch_batch_frame(upbd_batch* b, int nsub, bool visc) {
     BLAUNCH(b, K_DISP, kb_disp<<<G, BT, 0, st>>>(a));
     if (iters == 0) BLAUNCH(b, K_APPLY_FLUID, kb_apply_fluid<<<G, BT, 0, st>>>(a));
     if (scc) BLAUNCH(b, K_COLLECT, kb_collect_contacts<<<G, BT, 0, st>>>(a));
-    for (int it = 0; it < iters; it++) {
-      if (it == 0) BLAUNCH(b, K_SOLID_SOLVE, kb_solid_solve<true><<<G, BT, 0, st>>>(a));
-      else BLAUNCH(b, K_SOLID_SOLVE, kb_solid_solve<false><<<G, BT, 0, st>>>(a));
+    for (int it = 0; it < iters && fold; it++) {  // each iteration one launch (b_solid_solve's OUT)
+      if (it == 0) BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<true, SOLVE_STEP><<<G, BT, 0, st>>>(a, it)));
+      else if (it < iters - 1) BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<false, SOLVE_STEP><<<G, BT, 0, st>>>(a, it)));
+      else BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<false, SOLVE_LAST><<<G, BT, 0, st>>>(a, it)));
+    }
+    for (int it = 0; it < iters && !fold; it++) {
+      if (it == 0) BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<true, SOLVE_DELTA><<<G, BT, 0, st>>>(a, it)));
+      else BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<false, SOLVE_DELTA><<<G, BT, 0, st>>>(a, it)));
       if (mark_in_apply && it == iters - 1) BLAUNCH(b, K_APPLY_SOLID, kb_apply_solid<true><<<G, BT, 0, st>>>(a));
       else BLAUNCH(b, K_APPLY_SOLID, kb_apply_solid<false><<<G, BT, 0, st>>>(a));
       if (tets) {
@@ -449,8 +452,7 @@ int launch_batch_frame(upbd_batch* b, int nsub, bool visc) {
       BLAUNCH(b, K_SOLID_VISC, kb_solid_visc<<<G, BT, 0, st>>>(a));
       BLAUNCH(b, K_SOLID_VISC, kb_solid_visc_apply<<<G, BT, 0, st>>>(a));
     }
-    BLAUNCH(b, K_XSPH, kb_xsph<<<G, BT, 0, st>>>(a));
-    BLAUNCH(b, K_XSPH_APPLY, kb_xsph_apply<<<G, BT, 0, st>>>(a));
+    BLAUNCH(b, K_XSPH, kb_xsph<<<G, BT, 0, st>>>(a));  // writes the blended velocity itself
   }
   BLAUNCH(b, K_COUNT_ACTIVE, kb_count_active<<<G, BT, 0, st>>>(a));
   const cudaError_t e = cudaPeekAtLastError();

@@ -115,6 +115,7 @@ struct SimView {
   const uint32_t* adj_other;  // CSR-parallel: the other endpoint of constraint ids[k]
   const float* adj_scale;     // CSR-parallel: 1 / max(deg_i, deg_other) (static)
   uint32_t* mark;      // per particle: a solid is within contact range (fluid only)
+  float4* sbuf;        // 2 x S: solid positions between folded solve iterations
   uint32_t* ccount;
   uint32_t* clist;
   uint32_t* scratch;

@@ -68,9 +68,9 @@ __global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __rest
   b_disp(v, P, blockIdx.x);
 }
 __global__ void __launch_bounds__(256) k_apply_fluid(SimView v) { b_apply_fluid(v, blockIdx.x); }
-template <bool APPLY_FLUID>
-__global__ void __launch_bounds__(256) k_solid_solve(SimView v, const DevParams* __restrict__ P, int solid_pad) {
-  b_solid_solve<APPLY_FLUID>(v, P, solid_pad, blockIdx.x);
+template <bool APPLY_FLUID, int OUT>
+__global__ void __launch_bounds__(256) k_solid_solve(SimView v, const DevParams* __restrict__ P, int solid_pad, int it) {
+  b_solid_solve<APPLY_FLUID, OUT>(v, P, solid_pad, it, blockIdx.x);
 }
 template <bool MARK>
 __global__ void __launch_bounds__(256) k_apply_solid(SimView v, const DevParams* __restrict__ P) {
@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(256) k_solid_visc(SimView v, const DevParams* 
   b_solid_visc(v, P, blockIdx.x);
 }
 __global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) { b_solid_visc_apply(v, blockIdx.x); }
-__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) { b_xsph(v, P, blockIdx.x); }
-__global__ void __launch_bounds__(256) k_xsph_apply(SimView v) { b_xsph_apply(v, blockIdx.x); }
+template <bool APPLY>
+__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) { b_xsph<APPLY>(v, P, blockIdx.x); }
 __global__ void __launch_bounds__(256) k_count_active(SimView v) { b_count_active(v, blockIdx.x, gridDim.x); }
 
 // ------------------------------------------------------------------ tools

@@ -362,6 +362,25 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
 }
 
 // ------------------------------------------------------------------ solids
+// Marks the fluid particles within contact range of solid i at position p
+// (GL lanes per solid). The bound is widened by 1e-5 so the set only grows:
+// the contacts pass makes the exact test.
+// Every lane of the warp calls it (the hash is shared by shuffles); only
+// active solids walk.
+__device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, float4 p,
+                                                bool act, int lane) {
+  CellHash ch;
+  group_cell_hash(p.x, p.y, p.z, P->inv_cell, ch);
+  const float rsum = P->solid_radius + P->fluid_radius;
+  const float lim2 = rsum * rsum * 1.00001f;
+  const float4* __restrict__ spos = v.spos;
+  uint32_t* __restrict__ mark = v.mark;
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
+    const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+    if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
+  });
+}
+
 // solidSolve, src/gpu/wgsl.js:326-359, GL lanes per solid: lane l takes the
 // incident constraints k = st+l, st+l+GL, ... of the static CSR, whose other
 // endpoint and pair scale 1/max(deg_i, deg_j) are precomputed (both are fixed
@@ -369,8 +388,23 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
 // Threads from solid_pad on (a warp multiple, so the solve's warps are whole)
 // apply the fluid displacement when APPLY_FLUID (applyDeltaFluid,
 // src/gpu/wgsl.js:318-323): the solve reads solid positions only.
-template <bool APPLY_FLUID>
-__device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams* __restrict__ P, int solid_pad, uint32_t vb) {
+//
+// OUT selects what the solve does with solid i's correction:
+//   SOLVE_DELTA  writes delta[i] for b_apply_solid (the reference's split).
+//   SOLVE_STEP   applies it too (applyDeltaSolid, src/gpu/wgsl.js:361-366)
+//                into a ping-pong copy of the solid positions: iteration `it`
+//                reads pos (it 0) or sbuf[(it-1)&1] and writes sbuf[it&1],
+//                inactive solids carried over unchanged.
+//   SOLVE_LAST   applies it into pos and the slot copy, then marks the fluid
+//                near the final position (b_apply_solid<true>'s work).
+// Every solve reads the previous iteration's positions only, as with the
+// split passes, and pos + omega * delta is the same expression, so the
+// folded iterations give the split ones' results bit for bit; they need at
+// least two iterations (the first may not write what it reads).
+constexpr int SOLVE_DELTA = 0, SOLVE_STEP = 1, SOLVE_LAST = 2;
+template <bool APPLY_FLUID, int OUT = SOLVE_DELTA>
+__device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams* __restrict__ P, int solid_pad, int it,
+                                              uint32_t vb) {
   const int t = UPBD_VTID;
   if (t >= solid_pad) {
     const int i = v.S + (t - solid_pad);
@@ -386,16 +420,16 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
   const int i = t / GL;
   const int lane = threadIdx.x & (GL - 1);
   const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
+  const float4* __restrict__ pos = (OUT == SOLVE_DELTA || it == 0) ? v.pos : v.sbuf + (size_t)((it - 1) & 1) * v.S;
+  const float4 pi = (i < v.S) ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   float cx = 0.f, cy = 0.f, cz = 0.f;
   if (act) {
-    const float4 pi = v.pos[i];
     const float wi = pi.w;
     const float h = P->h;
     const float alpha = P->compliance / (h * h);
     const uint32_t st = v.adj[i], en = v.adj[i + 1];
     const uint32_t* __restrict__ ids = v.adj + v.S + 1;
     const uint4* __restrict__ cons = v.cons;
-    const float4* __restrict__ pos = v.pos;
 #pragma unroll 2
     for (uint32_t k = st + lane; k < en; k += GL) {
       const uint32_t ci = __ldg(&ids[k]);
@@ -418,26 +452,25 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
   cx = lane_sum(cx);
   cy = lane_sum(cy);
   cz = lane_sum(cz);
-  if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, 1.0f);
-}
-
-// Marks the fluid particles within contact range of solid i at position p
-// (GL lanes per solid). The bound is widened by 1e-5 so the set only grows:
-// the contacts pass makes the exact test.
-// Every lane of the warp calls it (the hash is shared by shuffles); only
-// active solids walk.
-__device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, float4 p,
-                                                bool act, int lane) {
-  CellHash ch;
-  group_cell_hash(p.x, p.y, p.z, P->inv_cell, ch);
-  const float rsum = P->solid_radius + P->fluid_radius;
-  const float lim2 = rsum * rsum * 1.00001f;
-  const float4* __restrict__ spos = v.spos;
-  uint32_t* __restrict__ mark = v.mark;
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
-    const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-    if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
-  });
+  if (OUT == SOLVE_DELTA) {
+    if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+    return;
+  }
+  // applyDeltaSolid on the correction just summed (the delta b_apply_solid reads)
+  const float w = P->omega;
+  float4 p = pi;
+  if (act) {
+    p.x = p.x + cx * w; p.y = p.y + cy * w; p.z = p.z + cz * w;
+  }
+  if (OUT == SOLVE_STEP) {
+    if (i < v.S && lane == 0) v.sbuf[(size_t)(it & 1) * v.S + i] = p;
+    return;
+  }
+  if (act && lane == 0) {
+    v.pos[i] = p;
+    v.spos[v.slot[i]] = p;
+  }
+  if (P->use_mark) mark_fluid_near(v, P, act ? p : make_float4(0.f, 0.f, 0.f, 0.f), act, lane);
 }
 
 // applyDeltaSolid, src/gpu/wgsl.js:361-366. With MARK (last iteration of the
@@ -894,7 +927,11 @@ __device__ __forceinline__ void b_solid_visc_apply(const SimView& v, uint32_t vb
 // xsph, src/gpu/wgsl.js:745-771 (slot-ordered groups, as b_density). The
 // grid still holds the particles bounds culled this substep: they are
 // neighbours (the reference does not test their flag) but have no pass of
-// their own.
+// their own. Neighbour velocities come from the slot copies (svel), so with
+// APPLY the blended velocity goes straight to vel[i] (xsphApply's result,
+// src/gpu/wgsl.js:773-778) and the copy pass is not needed; without it the
+// result waits in delta, where the reference's xsph pass leaves it.
+template <bool APPLY>
 __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GL - 1);
@@ -930,19 +967,12 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
       vy = vy + mu * (sy / m - vy);
       vz = vz + mu * (sz / m - vz);
     }
-    v.delta[i] = make_float4(vx, vy, vz, m);
+    if (APPLY)
+      v.vel[i] = make_float4(vx, vy, vz, 0.f);
+    else
+      v.delta[i] = make_float4(vx, vy, vz, m);
   }
 }
-
-// xsphApply, src/gpu/wgsl.js:773-778
-__device__ __forceinline__ void b_xsph_apply(const SimView& v, uint32_t vb) {
-  const int i = v.S + (int)UPBD_VTID;
-  if (i >= v.N) return;
-  if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 d = v.delta[i];
-  v.vel[i] = make_float4(d.x, d.y, d.z, 0.f);
-}
-
 
 // countActive (src/gpu/wgsl.js:874-879) with a last-block epilogue that
 // publishes the count and the health bits to mapped host memory.

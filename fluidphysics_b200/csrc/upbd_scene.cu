@@ -190,6 +190,7 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.ascl = cv.take<float>(std::max<size_t>(hs.adj_scale.size(), 1));
   L.ccount = cv.take<uint32_t>(scc ? std::max(v.S, 1) : 1);
   L.clist = cv.take<uint32_t>(scc ? (size_t)std::max(v.S, 1) * C_K : 1);
+  L.sbuf = cv.take<float4>(2 * (size_t)std::max(v.S, 1));
   L.scr = cv.take<uint32_t>(SCR_WORDS);
   L.par = cv.take<DevParams>(1);
   L.bytes = cv.off;
@@ -227,6 +228,7 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.adj_scale = (const float*)(base + L.ascl);
   v.ccount = (uint32_t*)(base + L.ccount);
   v.clist = (uint32_t*)(base + L.clist);
+  v.sbuf = (float4*)(base + L.sbuf);
   v.scratch = (uint32_t*)(base + L.scr);
   if (params) *params = (DevParams*)(base + L.par);
 }
