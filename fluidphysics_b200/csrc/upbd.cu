@@ -71,6 +71,10 @@ struct upbd_sim {
   size_t arena_bytes = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // second stream of the substep: the solid solve's first iterations run
+  // there beside the grid build and the fluid gathers (fork / join events)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   // host copies for reset
   std::vector<float4> init_pos;
   std::vector<uint4> init_cons;
@@ -174,7 +178,26 @@ int launch_substep(upbd_sim* s, int last) {
     UPBD_KCK(s);
     return UPBD_OK;
   }
+  // With two or more plain Jacobi iterations (no tets, no solid contacts)
+  // each iteration is one launch that also applies (b_solid_solve's OUT), and
+  // the displacement pass applies the fluid's move itself. The iterations
+  // before the last read and write solid positions only (pos, sbuf), which no
+  // pass of the grid build or the fluid gathers writes, so they run on the
+  // side stream meanwhile; the last one (slot copies, contact marks) waits
+  // for both. Eager per-kernel timing keeps one stream.
+  const bool fold = iters >= 2 && !tets && !scc && last >= UPBD_PASS_SOLID;
+  const bool overlap = fold && !s->prof_on && s->side;
+  const int solid_pad = ((v.S * GL + 31) / 32) * 32;  // lane threads of the solve, whole warps
   PROF(s, K_INTEGRATE, k_integrate_count<true, true><<<blocks_for(v.N), 256, 0, st>>>(v, P));
+  if (overlap) {
+    UPBD_CK(s, cudaEventRecord(s->fork_ev, st));
+    UPBD_CK(s, cudaStreamWaitEvent(s->side, s->fork_ev, 0));
+    for (int it = 0; it < iters - 1; it++) {
+      k_solid_solve<false, SOLVE_STEP><<<blocks_for(solid_pad), 256, 0, s->side>>>(v, P, solid_pad, it);
+      L++;
+    }
+    UPBD_CK(s, cudaEventRecord(s->join_ev, s->side));
+  }
   PROF(s, K_SCAN, k_scan<<<v.num_tiles, SCAN_THREADS, 0, st>>>(v));
   PROF(s, K_SCATTER, k_scatter<<<blocks_for(std::max(v.N, tile_words(v.num_tiles))), 256, 0, st>>>(v));
   PROF(s, K_RANKFIX, k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v));
@@ -185,11 +208,14 @@ int launch_substep(upbd_sim* s, int last) {
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_DISP) return UPBD_OK;
-  PROF(s, K_DISP, k_disp<<<blocks_for(fl), 256, 0, st>>>(v, P));
+  if (fold)
+    PROF(s, K_DISP, k_disp<true><<<blocks_for(fl), 256, 0, st>>>(v, P));
+  else
+    PROF(s, K_DISP, k_disp<false><<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   UPBD_KCK(s);
   if (last < UPBD_PASS_APPLY_FLUID) return UPBD_OK;
-  if (last < UPBD_PASS_SOLID || iters == 0) {
+  if (!fold && (last < UPBD_PASS_SOLID || iters == 0)) {
     PROF(s, K_APPLY_FLUID, k_apply_fluid<<<blocks_for(v.F), 256, 0, st>>>(v));
     L++;
     if (last < UPBD_PASS_SOLID) return UPBD_OK;
@@ -201,18 +227,17 @@ int launch_substep(upbd_sim* s, int last) {
   // the contact marks ride on the last applyDeltaSolid when that is the last
   // position update of the solve; otherwise they get their own launch
   const bool mark_in_apply = iters > 0 && !tets && !scc;
-  const int solid_pad = ((v.S * GL + 31) / 32) * 32;  // lane threads of the solve, whole warps
-  // with two or more plain iterations each one is a single launch that also
-  // applies (b_solid_solve's OUT); the last marks the fluid near the solids
-  const bool fold = iters >= 2 && !tets && !scc;
-  for (int it = 0; it < iters && fold; it++) {
-    if (it == 0)
-      PROF(s, K_SOLID_SOLVE, k_solid_solve<true, SOLVE_STEP>
-           <<<blocks_for((long long)solid_pad + v.F), 256, 0, st>>>(v, P, solid_pad, it));
-    else if (it < iters - 1)
-      PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_STEP><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));
-    else
-      PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_LAST><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));
+  if (fold) {
+    if (overlap) {
+      UPBD_CK(s, cudaStreamWaitEvent(st, s->join_ev, 0));
+    } else {
+      for (int it = 0; it < iters - 1; it++) {
+        PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_STEP><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));
+        L++;
+      }
+    }
+    PROF(s, K_SOLID_SOLVE,
+         k_solid_solve<false, SOLVE_LAST><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, iters - 1));
     L++;
   }
   for (int it = 0; it < iters && !fold; it++) {
@@ -467,6 +492,10 @@ int upbd_create(const upbd_scene_desc* desc, const upbd_params* params, upbd_sim
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup_fail(UPBD_ERR_CUDA, "stream creation failed");
   s->own_stream = true;
+  if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess)
+    return cleanup_fail(UPBD_ERR_CUDA, "side stream creation failed");
   if (cudaHostAlloc((void**)&s->stage, sizeof(DevParams) * kStageRing, cudaHostAllocDefault) != cudaSuccess)
     return cleanup_fail(UPBD_ERR_OOM, "pinned staging allocation failed");
   if (cudaHostAlloc((void**)&s->hmapped, sizeof(uint32_t) * HM_WORDS, cudaHostAllocMapped) != cudaSuccess)
@@ -514,6 +543,12 @@ int upbd_destroy(upbd_sim* s) {
   if (s->hmapped) cudaFreeHost(s->hmapped);
   if (s->arena) cudaFree(s->arena);
   if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
+  if (s->side) {
+    cudaStreamSynchronize(s->side);
+    cudaStreamDestroy(s->side);
+  }
+  if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+  if (s->join_ev) cudaEventDestroy(s->join_ev);
   delete s;
   return UPBD_OK;
 }

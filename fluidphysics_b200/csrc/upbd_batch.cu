@@ -109,8 +109,9 @@ __global__ void __launch_bounds__(256) kb_rankfix(BatchArgs a) {
 __global__ void __launch_bounds__(256) kb_density(BatchArgs a) {
   batch_loop<D_FGL, false>(a, UPBD_BODY { b_density(v, P, vb); });
 }
+template <bool APPLY>
 __global__ void __launch_bounds__(256) kb_disp(BatchArgs a) {
-  batch_loop<D_FGL, false>(a, UPBD_BODY { b_disp(v, P, vb); });
+  batch_loop<D_FGL, false>(a, UPBD_BODY { b_disp<APPLY>(v, P, vb); });
 }
 __global__ void __launch_bounds__(256) kb_apply_fluid(BatchArgs a) {
   batch_loop<D_F, false>(a, UPBD_BODY { b_apply_fluid(v, vb); });
@@ -423,12 +424,14 @@ int launch_batch_frame(upbd_batch* b, int nsub, bool visc) {
     BLAUNCH(b, K_SCATTER, kb_scatter<<<G, BT, 0, st>>>(a));
     BLAUNCH(b, K_RANKFIX, kb_rankfix<<<G, BT, 0, st>>>(a));
     BLAUNCH(b, K_DENSITY, kb_density<<<G, BT, 0, st>>>(a));
-    BLAUNCH(b, K_DISP, kb_disp<<<G, BT, 0, st>>>(a));
+    if (fold)  // the displacement pass applies the fluid's move (b_disp<true>)
+      BLAUNCH(b, K_DISP, kb_disp<true><<<G, BT, 0, st>>>(a));
+    else
+      BLAUNCH(b, K_DISP, kb_disp<false><<<G, BT, 0, st>>>(a));
     if (iters == 0) BLAUNCH(b, K_APPLY_FLUID, kb_apply_fluid<<<G, BT, 0, st>>>(a));
     if (scc) BLAUNCH(b, K_COLLECT, kb_collect_contacts<<<G, BT, 0, st>>>(a));
     for (int it = 0; it < iters && fold; it++) {  // each iteration one launch (b_solid_solve's OUT)
-      if (it == 0) BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<true, SOLVE_STEP><<<G, BT, 0, st>>>(a, it)));
-      else if (it < iters - 1) BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<false, SOLVE_STEP><<<G, BT, 0, st>>>(a, it)));
+      if (it < iters - 1) BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<false, SOLVE_STEP><<<G, BT, 0, st>>>(a, it)));
       else BLAUNCH(b, K_SOLID_SOLVE, (kb_solid_solve<false, SOLVE_LAST><<<G, BT, 0, st>>>(a, it)));
     }
     for (int it = 0; it < iters && !fold; it++) {

@@ -116,6 +116,10 @@ struct SimView {
   const float* adj_scale;     // CSR-parallel: 1 / max(deg_i, deg_other) (static)
   uint32_t* mark;      // per particle: a solid is within contact range (fluid only)
   float4* sbuf;        // 2 x S: solid positions between folded solve iterations
+  // Slot-ordered fluid positions after applyDeltaFluid: the contact passes
+  // (marks, solid-fluid contacts) read the fluid there, while spos keeps the
+  // positions the fluid gathers saw until the bounds pass rewrites it.
+  float4* sfp;
   uint32_t* ccount;
   uint32_t* clist;
   uint32_t* scratch;

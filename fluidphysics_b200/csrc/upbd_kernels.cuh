@@ -64,8 +64,9 @@ __global__ void __launch_bounds__(256) k_rankfix(SimView v) { b_rankfix(v, block
 __global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __restrict__ P) {
   b_density(v, P, blockIdx.x);
 }
+template <bool APPLY>
 __global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __restrict__ P) {
-  b_disp(v, P, blockIdx.x);
+  b_disp<APPLY>(v, P, blockIdx.x);
 }
 __global__ void __launch_bounds__(256) k_apply_fluid(SimView v) { b_apply_fluid(v, blockIdx.x); }
 template <bool APPLY_FLUID, int OUT>

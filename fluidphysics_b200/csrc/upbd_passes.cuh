@@ -271,7 +271,12 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   }
 }
 
-// fluidDisp, src/gpu/wgsl.js:281-316 (slot-ordered groups, as b_density)
+// fluidDisp, src/gpu/wgsl.js:281-316 (slot-ordered groups, as b_density).
+// With APPLY it also applies the displacement (applyDeltaFluid,
+// src/gpu/wgsl.js:318-323): pos[i] and the group's own sfp slot are written,
+// while every group reads neighbours from spos, so no read sees a moved
+// particle.
+template <bool APPLY>
 __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GL - 1);
@@ -345,7 +350,13 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
       const float f = maxTotal / sqrtf(s2);
       sx = sx * f; sy = sy * f; sz = sz * f;
     }
-    v.delta[i] = make_float4(sx, sy, sz, 1.0f);
+    if (APPLY) {  // pi is pos[i]: the grid build copied it and nothing moved it since
+      const float4 p = make_float4(pi.x + sx, pi.y + sy, pi.z + sz, pi.w);
+      v.pos[i] = p;
+      v.sfp[myslot] = p;
+    } else {
+      v.delta[i] = make_float4(sx, sy, sz, 1.0f);
+    }
   }
 }
 
@@ -358,7 +369,7 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
   const float4 d = v.delta[i];
   p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
   v.pos[i] = p;
-  v.spos[v.slot[i]] = p;
+  v.sfp[v.slot[i]] = p;
 }
 
 // ------------------------------------------------------------------ solids
@@ -373,9 +384,9 @@ __device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParam
   group_cell_hash(p.x, p.y, p.z, P->inv_cell, ch);
   const float rsum = P->solid_radius + P->fluid_radius;
   const float lim2 = rsum * rsum * 1.00001f;
-  const float4* __restrict__ spos = v.spos;
+  const float4* __restrict__ sfp = v.sfp;  // the fluid has moved by its displacement
   uint32_t* __restrict__ mark = v.mark;
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return sfp[e]; }, [&](uint32_t e, const float4& pj) {
     const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
     if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
   });
@@ -413,7 +424,7 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
       const float4 d = v.delta[i];
       p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
       v.pos[i] = p;
-      v.spos[v.slot[i]] = p;
+      v.sfp[v.slot[i]] = p;
     }
     return;
   }
@@ -754,7 +765,9 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   const float ri = iSolid ? rs : rf;
   const float rsum = ri + (iSolid ? rf : rs);
   const float4* __restrict__ spos = v.spos;
-  auto load = [&](uint32_t e) { return spos[e]; };
+  const float4* __restrict__ sfp = v.sfp;
+  auto load_fluid = [&](uint32_t e) { return sfp[e]; };  // after the displacement
+  auto load_solid = [&](uint32_t e) { return spos[e]; };  // after the solve
   auto pair = [&](uint32_t, const float4& pj) {
     const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -774,8 +787,8 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   // a warp holds solids or fluid or both (at the S boundary): the two walks
   // are separate calls, each with every lane of the warp
   const unsigned FULL = 0xffffffffu;
-  if (__any_sync(FULL, walk && iSolid)) lane_strided<0>(v, ch, lane, walk && iSolid, load, pair);
-  if (__any_sync(FULL, walk && !iSolid)) lane_strided<1>(v, ch, lane, walk && !iSolid, load, pair);
+  if (__any_sync(FULL, walk && iSolid)) lane_strided<0>(v, ch, lane, walk && iSolid, load_fluid, pair);
+  if (__any_sync(FULL, walk && !iSolid)) lane_strided<1>(v, ch, lane, walk && !iSolid, load_solid, pair);
   cx = lane_sum(cx);
   cy = lane_sum(cy);
   cz = lane_sum(cz);

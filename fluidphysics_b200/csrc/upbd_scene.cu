@@ -191,6 +191,7 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.ccount = cv.take<uint32_t>(scc ? std::max(v.S, 1) : 1);
   L.clist = cv.take<uint32_t>(scc ? (size_t)std::max(v.S, 1) * C_K : 1);
   L.sbuf = cv.take<float4>(2 * (size_t)std::max(v.S, 1));
+  L.sfp = cv.take<float4>(v.N);
   L.scr = cv.take<uint32_t>(SCR_WORDS);
   L.par = cv.take<DevParams>(1);
   L.bytes = cv.off;
@@ -229,6 +230,7 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.ccount = (uint32_t*)(base + L.ccount);
   v.clist = (uint32_t*)(base + L.clist);
   v.sbuf = (float4*)(base + L.sbuf);
+  v.sfp = (float4*)(base + L.sfp);
   v.scratch = (uint32_t*)(base + L.scr);
   if (params) *params = (DevParams*)(base + L.par);
 }
