@@ -226,6 +226,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   uint32_t myslot, i;
   bool act;
   slot_group(v, t, myslot, i, act);
+  if (!__any_sync(0xffffffffu, act)) return;  // a warp of solid slots (or past the active count)
   float rho = 0.f, rhoNear = 0.f;
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
@@ -283,6 +284,7 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
   uint32_t myslot, i;
   bool act;
   slot_group(v, t, myslot, i, act);
+  if (!__any_sync(0xffffffffu, act)) return;
   const float H = P->fluid_h, H2 = H * H;
   float sx = 0.f, sy = 0.f, sz = 0.f;
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -754,6 +756,11 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   const bool act = i < nc && (v.flags[i] & F_ACTIVE);
   const bool iSolid = i < v.S;
   const bool walk = act && (iSolid || !P->use_mark || v.mark[i] != 0u);
+  const unsigned FULL = 0xffffffffu;
+  if (!__any_sync(FULL, walk)) {  // most fluid warps: nothing near a solid, no hash to compute
+    if (act && lane == 0) v.delta[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
   float cx = 0.f, cy = 0.f, cz = 0.f, cnt = 0.f;
   const float4 pi = walk ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
@@ -786,7 +793,6 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   };
   // a warp holds solids or fluid or both (at the S boundary): the two walks
   // are separate calls, each with every lane of the warp
-  const unsigned FULL = 0xffffffffu;
   if (__any_sync(FULL, walk && iSolid)) lane_strided<0>(v, ch, lane, walk && iSolid, load_fluid, pair);
   if (__any_sync(FULL, walk && !iSolid)) lane_strided<1>(v, ch, lane, walk && !iSolid, load_solid, pair);
   cx = lane_sum(cx);
@@ -952,6 +958,7 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   bool fluid;
   slot_group(v, t, myslot, i, fluid);
   const bool act = fluid && (v.flags[i] & F_ACTIVE);
+  if (!__any_sync(0xffffffffu, act)) return;
   float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
