@@ -208,10 +208,10 @@ int launch_substep(upbd_sim* s, int last) {
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_DISP) return UPBD_OK;
-  if (fold)
-    PROF(s, K_DISP, k_disp<true><<<blocks_for(fl), 256, 0, st>>>(v, P));
+  if (fold)  // DL threads per slot
+    PROF(s, K_DISP, k_disp<true><<<blocks_for((long long)v.N * DL), 256, 0, st>>>(v, P));
   else
-    PROF(s, K_DISP, k_disp<false><<<blocks_for(fl), 256, 0, st>>>(v, P));
+    PROF(s, K_DISP, k_disp<false><<<blocks_for((long long)v.N * DL), 256, 0, st>>>(v, P));
   L++;
   UPBD_KCK(s);
   if (last < UPBD_PASS_APPLY_FLUID) return UPBD_OK;

@@ -39,7 +39,8 @@ enum Domain {
   D_N,        // particles (integrate/count, rankfix, apply+bounds+velocity)
   D_TILES,    // scan tiles of the bucket table (SCAN_THREADS per block)
   D_SCATTER,  // max(particles, scan tiles)
-  D_FGL,      // GL lanes per grid slot (density, displacement, xsph)
+  D_FGL,      // GL lanes per grid slot (density, xsph)
+  D_DISP,     // DL threads per grid slot (displacement)
   D_F,        // fluid particles (apply, xsph apply, active count)
   D_SOLVE0,   // solve lanes rounded to warps + fluid (first iteration)
   D_SOLVE,    // solve lanes rounded to warps
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(256) kb_density(BatchArgs a) {
 }
 template <bool APPLY>
 __global__ void __launch_bounds__(256) kb_disp(BatchArgs a) {
-  batch_loop<D_FGL, false>(a, UPBD_BODY { b_disp<APPLY>(v, P, vb); });
+  batch_loop<D_DISP, false>(a, UPBD_BODY { b_disp<APPLY>(v, P, vb); });
 }
 __global__ void __launch_bounds__(256) kb_apply_fluid(BatchArgs a) {
   batch_loop<D_F, false>(a, UPBD_BODY { b_apply_fluid(v, vb); });
@@ -182,6 +183,7 @@ void scene_blocks(const SimView& v, bool tets, int bt, uint32_t out[NUM_DOMAINS]
   out[D_TILES] = (uint32_t)std::max(v.num_tiles, 1);
   out[D_SCATTER] = ceil_div(std::max(v.N, tile_words(v.num_tiles)), bt);
   out[D_FGL] = ceil_div((long long)v.N * GL, bt);
+  out[D_DISP] = ceil_div((long long)v.N * DL, bt);
   out[D_F] = ceil_div(v.F, bt);
   out[D_SOLVE0] = ceil_div((long long)sp + v.F, bt);
   out[D_SOLVE] = ceil_div(sp, bt);

@@ -107,9 +107,9 @@ struct SimView {
   // precede solids: fend[h] splits bucket h into [start[h], fend[h]) fluid and
   // [fend[h], start[h+1]) solid.
   uint32_t* fend;
-  // Density-pass neighbour lists: lane g = e*GL + l of the fluid particle at
-  // slot e records the slots of its in-range fluid neighbours, in walk order,
-  // at nbr[c * N*GL + g] (c < NL), and their number in ncount[g].
+  // Density-pass neighbour lists: lane l of the fluid particle at slot e
+  // records the slots of its in-range fluid neighbours, in its walk order, at
+  // nbr[(l*NL + c) * N + e] (c < NL), and their number in ncount[l*N + e].
   uint32_t* nbr;
   uint32_t* ncount;
   const uint32_t* adj_other;  // CSR-parallel: the other endpoint of constraint ids[k]
@@ -176,6 +176,7 @@ struct CellHash {
 // result is deterministic: ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
 constexpr int GL = 8;
 constexpr uint32_t NL = 16;  // neighbour-list entries kept per lane
+constexpr int DL = 2;        // threads per particle in the displacement pass
 
 __device__ __forceinline__ float lane_sum(float x) {
   x = x + __shfl_xor_sync(0xffffffffu, x, 4);

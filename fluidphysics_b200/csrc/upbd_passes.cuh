@@ -233,9 +233,9 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
   const float H = P->fluid_h, H2 = H * H;
   const float4* __restrict__ spos = v.spos;
-  const uint32_t NG = (uint32_t)v.N * GL;
-  const uint32_t g = myslot * GL + lane;
-  uint32_t* __restrict__ nbr = v.nbr + g;
+  // lane l's c-th in-range neighbour goes to row l*NL + c, column myslot
+  const uint32_t NS = (uint32_t)v.N;
+  uint32_t* __restrict__ nbr = v.nbr + (size_t)lane * NL * NS + myslot;
   uint32_t cnt = 0;
 #ifndef UPBD_PARITY_BUILD
   const float invH = 1.0f / H;
@@ -249,7 +249,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
     const float q = 1.0f - sqrtf(d2) / H;
     rho = rho + q * q;
     rhoNear = rhoNear + q * q * q;
-    if (cnt < NL) nbr[cnt * NG] = e;  // for fluidDisp, same positions
+    if (cnt < NL) nbr[cnt * NS] = e;  // for fluidDisp, same positions
     cnt++;
 #else
     // branch-free: every lane of the warp takes the same path per candidate
@@ -258,11 +258,11 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
     const float qq = in ? q * q : 0.0f;
     rho = rho + qq;
     rhoNear = rhoNear + qq * q;
-    if (in && cnt < NL) nbr[cnt * NG] = e;  // for fluidDisp, same positions
+    if (in && cnt < NL) nbr[cnt * NS] = e;  // for fluidDisp, same positions
     cnt += in ? 1u : 0u;
 #endif
   });
-  if (act) v.ncount[g] = cnt;
+  if (act) v.ncount[lane * NS + myslot] = cnt;
   rho = lane_sum(rho);
   rhoNear = lane_sum(rhoNear);
   if (act && lane == 0) {
@@ -272,93 +272,132 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   }
 }
 
-// fluidDisp, src/gpu/wgsl.js:281-316 (slot-ordered groups, as b_density).
-// With APPLY it also applies the displacement (applyDeltaFluid,
-// src/gpu/wgsl.js:318-323): pos[i] and the group's own sfp slot are written,
-// while every group reads neighbours from spos, so no read sees a moved
-// particle.
+// fluidDisp, src/gpu/wgsl.js:281-316, DL threads per slot over the density
+// pass's lists (same positions). Thread h of a slot takes lanes h*GL/DL ..
+// (h+1)*GL/DL - 1: lane l's in-range neighbours in its walk order, then the
+// next lane's, summed one after another; the DL partials combine by the xor
+// butterfly. A thread whose lists overflowed walks the 27 buckets for its
+// lanes' shares instead, in the same order. With APPLY it also applies the
+// displacement (applyDeltaFluid, src/gpu/wgsl.js:318-323): pos[i] and the own
+// sfp slot are written, while every thread reads neighbours from spos, so no
+// read sees a moved particle.
 template <bool APPLY>
 __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
-  const uint32_t t = UPBD_VTID;
-  const int lane = threadIdx.x & (GL - 1);
-  uint32_t myslot, i;
-  bool act;
-  slot_group(v, t, myslot, i, act);
-  if (!__any_sync(0xffffffffu, act)) return;
+  constexpr int LPT = GL / DL;  // lanes' lists per thread
+  const uint32_t e0 = UPBD_VTID / DL;
+  const int h = (int)(threadIdx.x & (DL - 1));
+  const uint32_t nact = __ldg(&v.start[v.T]);
+  const uint32_t i = (e0 < nact) ? v.entries[e0] : 0u;
+  const bool act = e0 < nact && i >= (uint32_t)v.S;
+  if (DL > 1) {
+    if (!__any_sync(0xffffffffu, act)) return;
+  } else if (!act) {
+    return;
+  }
   const float H = P->fluid_h, H2 = H * H;
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const uint32_t NG = (uint32_t)v.N * GL;
-  const uint32_t g = myslot * GL + lane;
-  const uint32_t cnt = act ? v.ncount[g] : 0u;
-  const float maxPair = 0.05f * H;
-  const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
-  const float2 di = act ? v.sdens[myslot] : make_float2(0.f, 0.f);
-  const float Pi = k * (di.x - rho0);
-  const float PNi = kn * di.y;
   const float4* __restrict__ spos = v.spos;
   const float2* __restrict__ sdens = v.sdens;
+  const float4 pi = act ? spos[e0] : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (act) {
+    const float maxPair = 0.05f * H;
+    const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
+    const float2 di = sdens[e0];
+    const float Pi = k * (di.x - rho0);
+    const float PNi = kn * di.y;
 #ifndef UPBD_PARITY_BUILD
-  const float invH = 1.0f / H;
+    const float invH = 1.0f / H;
 #endif
-  auto pair = [&](const float4& pj, const float2& dj) {
-    const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-    if (d2 >= H2 || d2 < 1e-12f) return;
+    auto pair = [&](const float4& pj, const float2& dj) {
+      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      if (d2 >= H2 || d2 < 1e-12f) return;
 #ifdef UPBD_PARITY_BUILD
-    const float d = sqrtf(d2);
-    const float q = 1.0f - d / H;
+      const float d = sqrtf(d2);
+      const float q = 1.0f - d / H;
 #else
-    const float rd = rsqrtf(d2);  // d2 >= 1e-12 here
-    const float d = d2 * rd;
-    const float q = 1.0f - d * invH;
+      const float rd = rsqrtf(d2);  // d2 >= 1e-12 here
+      const float d = d2 * rd;
+      const float q = 1.0f - d * invH;
 #endif
-    const float Pj = k * (dj.x - rho0);
-    const float PNj = kn * dj.y;
-    float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
-    D = clampf(D, -maxPair, maxPair);
+      const float Pj = k * (dj.x - rho0);
+      const float PNj = kn * dj.y;
+      float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
+      D = clampf(D, -maxPair, maxPair);
 #ifdef UPBD_PARITY_BUILD
-    const float f = D / d;
+      const float f = D / d;
 #else
-    const float f = D * rd;
+      const float f = D * rd;
 #endif
-    sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
-  };
-  // the density pass listed this lane's in-range neighbours at these same
-  // positions and in walk order; a lane whose list overflowed walks its
-  // share again (the whole warp takes part in the walk's shuffles)
-  const bool over = act && cnt > NL;
-  if (act && !over) {
-    const uint32_t* __restrict__ nbr = v.nbr + g;
-    for (uint32_t c = 0; c < cnt; c++) {
-      const uint32_t e = __ldg(&nbr[c * NG]);
-      pair(spos[e], sdens[e]);
+      sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
+    };
+    const uint32_t NS = (uint32_t)v.N;
+    const int l0 = h * LPT;
+    uint32_t cnt[LPT];
+    bool over = false;
+#pragma unroll
+    for (int u = 0; u < LPT; u++) {
+      cnt[u] = v.ncount[(l0 + u) * NS + e0];
+      over = over || cnt[u] > NL;
     }
-  }
-  if (__any_sync(0xffffffffu, over)) {
-    CellHash ch;
-    group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-    lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
-      if (over && e != myslot) pair(pj, sdens[e]);
-    });
-  }
-  sx = lane_sum(sx);
-  sy = lane_sum(sy);
-  sz = lane_sum(sz);
-  if (act && lane == 0) {
-    const float maxTotal = 0.35f * H;
-    const float s2 = dot3(sx, sy, sz, sx, sy, sz);
-    if (s2 > maxTotal * maxTotal) {
-      const float f = maxTotal / sqrtf(s2);
-      sx = sx * f; sy = sy * f; sz = sz * f;
-    }
-    if (APPLY) {  // pi is pos[i]: the grid build copied it and nothing moved it since
-      const float4 p = make_float4(pi.x + sx, pi.y + sy, pi.z + sz, pi.w);
-      v.pos[i] = p;
-      v.sfp[myslot] = p;
+    if (!over) {
+      const uint32_t* __restrict__ nbr = v.nbr + e0;
+#pragma unroll
+      for (int u = 0; u < LPT; u++) {
+        // four entries at a time: their list, position and density loads are
+        // in flight together (a lane list holds ~4)
+        for (uint32_t c = 0; c < cnt[u]; c += 4) {
+          uint32_t e[4];
+          float4 pj[4];
+          float2 dj[4];
+#pragma unroll
+          for (int w = 0; w < 4; w++)
+            e[w] = (c + w < cnt[u]) ? __ldg(&nbr[((uint32_t)(l0 + u) * NL + c + w) * NS]) : e0;
+#pragma unroll
+          for (int w = 0; w < 4; w++) {
+            pj[w] = spos[e[w]];
+            dj[w] = sdens[e[w]];
+          }
+#pragma unroll
+          for (int w = 0; w < 4; w++)
+            if (c + w < cnt[u]) pair(pj[w], dj[w]);
+        }
+      }
     } else {
-      v.delta[i] = make_float4(sx, sy, sz, 1.0f);
+      // lane l's share of the walk: candidates c = l, l+GL, ... of the sequence
+      CellHash ch;
+      ch.init(pi.x, pi.y, pi.z, P->inv_cell);
+      const uint32_t mask = (uint32_t)v.T - 1u;
+      for (int l = l0; l < l0 + LPT; l++) {
+        uint32_t c = 0;
+        for (int kk = 0; kk < 27; kk++) {
+          const uint32_t hb = ch.bucket_k(kk, mask);
+          const uint32_t s0 = __ldg(&v.start[hb]), s1 = __ldg(&v.fend[hb]);
+          for (uint32_t e = s0; e < s1; e++, c++)
+            if ((c & (GL - 1)) == (uint32_t)l && e != e0) pair(spos[e], sdens[e]);
+        }
+      }
     }
+  }
+#pragma unroll
+  for (int d = DL / 2; d > 0; d >>= 1) {
+    sx = sx + __shfl_xor_sync(0xffffffffu, sx, d);
+    sy = sy + __shfl_xor_sync(0xffffffffu, sy, d);
+    sz = sz + __shfl_xor_sync(0xffffffffu, sz, d);
+  }
+  if (!act || h != 0) return;
+  const float maxTotal = 0.35f * H;
+  const float s2 = dot3(sx, sy, sz, sx, sy, sz);
+  if (s2 > maxTotal * maxTotal) {
+    const float f = maxTotal / sqrtf(s2);
+    sx = sx * f; sy = sy * f; sz = sz * f;
+  }
+  if (APPLY) {  // pi is pos[i]: the grid build copied it and nothing moved it since
+    const float4 p = make_float4(pi.x + sx, pi.y + sy, pi.z + sz, pi.w);
+    v.pos[i] = p;
+    v.sfp[e0] = p;
+  } else {
+    v.delta[i] = make_float4(sx, sy, sz, 1.0f);
   }
 }
 

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <vector>
 
 #include "js_numerics.h"
 
@@ -36,7 +37,10 @@ static constexpr uint32_t C_K = 40u;  // src/gpu/wgsl.js:25
 // (dz+1) in order and each bucket's entries in order, form one sequence c =
 // 0, 1, ...; candidate c goes to lane c mod GL (GL = 8), every lane sums from
 // zero, and the eight partials combine as ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
+// fluidDisp instead sums the lanes' shares in lane order, DL partial sums of
+// GL/DL lanes each, combined by the same kind of butterfly.
 static constexpr int GL = 8;
+static constexpr int DL = 2;  // fluidDisp threads per particle
 template <class R> static inline R lane_reduce(const R* p) {
   return ((p[0] + p[4]) + (p[2] + p[6])) + ((p[1] + p[5]) + (p[3] + p[7]));
 }
@@ -375,22 +379,37 @@ template <class R> void O2Sim<R>::passDisp() {
     const V4<R> pi = pos[i];
     const R Pi = P.stiffness * (density[i].x - P.restDensity);
     const R PNi = P.nearStiffness * density[i].y;
-    R px[GL] = {}, py[GL] = {}, pz[GL] = {};
+    // DL sums over the neighbours in lane-major order: part h takes lanes
+    // h*GL/DL .. (h+1)*GL/DL - 1, lane l's share of the walk being candidates
+    // c = l, l+GL, ... (the CUDA pass reads them from the density pass's
+    // per-lane lists in that order); the parts combine by the xor butterfly
+    std::vector<uint32_t> share[GL];
     strided_walk(*this, pi, false, [&](int l, uint32_t j) {
-      if (j == (uint32_t)i || j < (uint32_t)S) return;
-      const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
-      const R d2 = dot3(ex, ey, ez, ex, ey, ez);
-      if (d2 >= H2 || d2 < LIT(1e-12)) return;
-      const R d = std::sqrt(d2);
-      const R q = LIT(1.0) - d / H;
-      const R Pj = P.stiffness * (density[j].x - P.restDensity);
-      const R PNj = P.nearStiffness * density[j].y;
-      R D = LIT(0.25) * ((Pi + Pj) * q + (PNi + PNj) * q * q);
-      D = clampR(D, -maxPair, maxPair);
-      const R f = D / d;
-      px[l] = px[l] - ex * f; py[l] = py[l] - ey * f; pz[l] = pz[l] - ez * f;
+      if (j != (uint32_t)i && j >= (uint32_t)S) share[l].push_back(j);
     });
-    R sx = lane_reduce(px), sy = lane_reduce(py), sz = lane_reduce(pz);
+    R part[DL][3] = {};
+    for (int l = 0; l < GL; l++) {
+      R& sx = part[l / (GL / DL)][0];
+      R& sy = part[l / (GL / DL)][1];
+      R& sz = part[l / (GL / DL)][2];
+      for (uint32_t j : share[l]) {
+        const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
+        const R d2 = dot3(ex, ey, ez, ex, ey, ez);
+        if (d2 >= H2 || d2 < LIT(1e-12)) continue;
+        const R d = std::sqrt(d2);
+        const R q = LIT(1.0) - d / H;
+        const R Pj = P.stiffness * (density[j].x - P.restDensity);
+        const R PNj = P.nearStiffness * density[j].y;
+        R D = LIT(0.25) * ((Pi + Pj) * q + (PNi + PNj) * q * q);
+        D = clampR(D, -maxPair, maxPair);
+        const R f = D / d;
+        sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
+      }
+    }
+    for (int dd = DL / 2; dd > 0; dd /= 2)  // the CUDA pass's xor butterfly
+      for (int a = 0; a < dd; a++)
+        for (int c = 0; c < 3; c++) part[a][c] = part[a][c] + part[a + dd][c];
+    R sx = part[0][0], sy = part[0][1], sz = part[0][2];
     const R s2 = dot3(sx, sy, sz, sx, sy, sz);
     if (s2 > maxTotal * maxTotal) {
       const R f = maxTotal / std::sqrt(s2);
