@@ -398,6 +398,32 @@ def run_served(args, batched: dict | None) -> dict:
     }
 
 
+def settled_capture(frames: int) -> None:
+    """Steps the default scene `frames` frames, then runs 3 more between
+    cudaProfilerStart and cudaProfilerStop: the settled-state window that the
+    launch lists and kernel captures under profiles/ are taken on."""
+    import torch
+    from fluidphysics_b200 import scenes as S
+    from fluidphysics_b200.sim import sim_from_scene
+
+    sc = S.gpu_default(frames=frames + 3)
+    sim = sim_from_scene(sc)
+    for k in range(frames):
+        if k == sc.slice_frame:
+            sim.slice(*sc.wedge)
+        sim.step(sc.dt, sc.substeps)
+    sim.sync()
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    for _ in range(3):
+        sim.step(sc.dt, sc.substeps)
+    sim.sync()
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    sim.close()
+    print(json.dumps({"settled_capture_frames": frames, "captured_frames": 3}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,11 +443,18 @@ def main() -> None:
                     help="seconds of Poisson arrivals served (0 skips the served line)")
     ap.add_argument("--large-frames", type=int, default=120,
                     help="timed frames of the large scene (0 skips the large line)")
+    ap.add_argument("--settled-capture", type=int, default=0,
+                    help="profiling mode: step the default scene this many frames on its graph (slice "
+                         "at frame 60), bracket the next 3 frames with cudaProfilerStart/Stop for "
+                         "ncu --profile-from-start off, and exit (no bench line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.settled_capture > 0:
+        settled_capture(args.settled_capture)
         return
 
     import torch
