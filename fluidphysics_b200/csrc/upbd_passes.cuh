@@ -1005,13 +1005,17 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   const float H = P->fluid_h, H2 = H * H;
   const float4* __restrict__ spos = v.spos;
   const float4* __restrict__ svel = v.svel;
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
-    if (e == myslot) return;
-    const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-    if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
-    const float4 vj = svel[e];
-    sx = sx + vj.x; sy = sy + vj.y; sz = sz + vj.z;
-    m = m + 1.0f;
+  // position and velocity of every candidate are loaded together, before the
+  // range test, and out-of-range ones add zero (the sums start at +0, so +0
+  // leaves them unchanged): no load waits on the test
+  struct PV {
+    float4 p, v;
+  };
+  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return PV{spos[e], svel[e]}; }, [&](uint32_t e, const PV& c) {
+    const float ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
+    const bool in = (e != myslot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
+    sx = sx + (in ? c.v.x : 0.f); sy = sy + (in ? c.v.y : 0.f); sz = sz + (in ? c.v.z : 0.f);
+    m = m + (in ? 1.0f : 0.f);
   });
   sx = lane_sum(sx);
   sy = lane_sum(sy);
