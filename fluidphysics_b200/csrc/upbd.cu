@@ -204,7 +204,7 @@ int launch_substep(upbd_sim* s, int last) {
   L += 4;
   UPBD_KCK(s);
   if (last < UPBD_PASS_DENSITY) return UPBD_OK;
-  const long long fl = (long long)v.N * GL;  // lane-parallel gathers over the slots
+  const long long fl = (long long)v.N * GLF;  // lane-parallel fluid gathers over the slots
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_DISP) return UPBD_OK;
@@ -292,11 +292,11 @@ int launch_substep(upbd_sim* s, int last) {
   }
   if (last < UPBD_PASS_XSPH) return UPBD_OK;
   if (last < UPBD_PASS_XSPH_APPLY) {  // stop with the result in delta, as the reference's xsph pass leaves it
-    PROF(s, K_XSPH, k_xsph<false><<<blocks_for((long long)v.N * GL), 256, 0, st>>>(v, P));
+    PROF(s, K_XSPH, k_xsph<false><<<blocks_for((long long)v.N * GLF), 256, 0, st>>>(v, P));
     L++;
     return UPBD_OK;
   }
-  PROF(s, K_XSPH, k_xsph<true><<<blocks_for((long long)v.N * GL), 256, 0, st>>>(v, P));
+  PROF(s, K_XSPH, k_xsph<true><<<blocks_for((long long)v.N * GLF), 256, 0, st>>>(v, P));
   L++;
   UPBD_KCK(s);
   return UPBD_OK;

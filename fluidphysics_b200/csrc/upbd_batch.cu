@@ -39,7 +39,7 @@ enum Domain {
   D_N,        // particles (integrate/count, rankfix, apply+bounds+velocity)
   D_TILES,    // scan tiles of the bucket table (SCAN_THREADS per block)
   D_SCATTER,  // max(particles, scan tiles)
-  D_FGL,      // GL lanes per grid slot (density, xsph)
+  D_FGL,      // GLF lanes per grid slot (density, xsph)
   D_DISP,     // DL threads per grid slot (displacement)
   D_F,        // fluid particles (apply, xsph apply, active count)
   D_SOLVE0,   // solve lanes rounded to warps + fluid (first iteration)
@@ -182,7 +182,7 @@ void scene_blocks(const SimView& v, bool tets, int bt, uint32_t out[NUM_DOMAINS]
   out[D_N] = ceil_div(v.N, bt);
   out[D_TILES] = (uint32_t)std::max(v.num_tiles, 1);
   out[D_SCATTER] = ceil_div(std::max(v.N, tile_words(v.num_tiles)), bt);
-  out[D_FGL] = ceil_div((long long)v.N * GL, bt);
+  out[D_FGL] = ceil_div((long long)v.N * GLF, bt);
   out[D_DISP] = ceil_div((long long)v.N * DL, bt);
   out[D_F] = ceil_div(v.F, bt);
   out[D_SOLVE0] = ceil_div((long long)sp + v.F, bt);

@@ -107,9 +107,10 @@ struct SimView {
   // precede solids: fend[h] splits bucket h into [start[h], fend[h]) fluid and
   // [fend[h], start[h+1]) solid.
   uint32_t* fend;
-  // Density-pass neighbour lists: lane l of the fluid particle at slot e
-  // records the slots of its in-range fluid neighbours, in its walk order, at
-  // nbr[(l*NL + c) * N + e] (c < NL), and their number in ncount[l*N + e].
+  // Density-pass neighbour lists: lane l (of GLF) of the fluid particle at
+  // slot e records the slots of its in-range fluid neighbours, in its walk
+  // order, at nbr[(l*NL + c) * N + e] (c < NL), and their number in
+  // ncount[l*N + e].
   uint32_t* nbr;
   uint32_t* ncount;
   const uint32_t* adj_other;  // CSR-parallel: the other endpoint of constraint ids[k]
@@ -170,73 +171,83 @@ struct CellHash {
   }
 };
 
-// Neighbour gathers run GL lanes per particle (lane_strided below deals the
+// Neighbour gathers run G lanes per particle (lane_strided below deals the
 // candidates to the lanes); each lane accumulates its own partial sums from
-// zero and the GL partials are combined by a fixed xor butterfly, so the
-// result is deterministic: ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
+// zero and the G partials are combined by a fixed xor butterfly, so the
+// result is deterministic: for G = 8 ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)),
+// for G = 4 (p0+p2) + (p1+p3). The contact gathers and the solid solve use
+// GL = 8 lanes; the fluid-fluid gathers (density, xsph) GLF = 4: each lane
+// walks the whole 27-cell sequence, so fewer lanes per particle cross fewer
+// cell boundaries in all.
 constexpr int GL = 8;
-constexpr uint32_t NL = 16;  // neighbour-list entries kept per lane
+constexpr int GLF = 4;
+constexpr uint32_t NL = 32;  // density-pass neighbour-list entries kept per fluid lane (GLF * NL per particle)
 constexpr int DL = 2;        // threads per particle in the displacement pass
 
+template <int G = GL>
 __device__ __forceinline__ float lane_sum(float x) {
-  x = x + __shfl_xor_sync(0xffffffffu, x, 4);
-  x = x + __shfl_xor_sync(0xffffffffu, x, 2);
-  x = x + __shfl_xor_sync(0xffffffffu, x, 1);
+#pragma unroll
+  for (int d = G / 2; d > 0; d >>= 1) x = x + __shfl_xor_sync(0xffffffffu, x, d);
   return x;
 }
 
 // The nine hash components of the cells around p (CellHash::init's values),
-// computed two per lane of a GL group and exchanged by shuffles. Every lane of
-// the warp must call it (inactive groups pass any position).
+// component j computed by lane j mod G of a G-lane group and exchanged by
+// shuffles. Every lane of the warp must call it (inactive groups pass any
+// position).
+template <int G = GL>
 __device__ __forceinline__ void group_cell_hash(float px, float py, float pz, double inv, CellHash& ch) {
   const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & (GL - 1);
-  const int base = (threadIdx.x & 31) & ~(GL - 1);
-  // lane l holds component l: x offsets -1..1 (lanes 0-2), y (3-5), z -1, 0 (6-7)
-  const int axis = lane / 3;
-  const float pa = (axis == 0) ? px : ((axis == 1) ? py : pz);
-  const double K = (axis == 0) ? 92837111.0 : ((axis == 1) ? 689287499.0 : 283923481.0);
-  const double c = floor(__dmul_rn((double)pa, inv));
-  const int32_t v1 = js_toint32(__dmul_rn(__dadd_rn(c, (double)(lane - 3 * axis - 1)), K));
-  // z offset +1, taken from the group's first lane
-  const double cz = floor(__dmul_rn((double)pz, inv));
-  const int32_t v2 = js_toint32(__dmul_rn(__dadd_rn(cz, 1.0), 283923481.0));
-  ch.hx[0] = __shfl_sync(FULL, v1, base + 0);
-  ch.hx[1] = __shfl_sync(FULL, v1, base + 1);
-  ch.hx[2] = __shfl_sync(FULL, v1, base + 2);
-  ch.hy[0] = __shfl_sync(FULL, v1, base + 3);
-  ch.hy[1] = __shfl_sync(FULL, v1, base + 4);
-  ch.hy[2] = __shfl_sync(FULL, v1, base + 5);
-  ch.hz[0] = __shfl_sync(FULL, v1, base + 6);
-  ch.hz[1] = __shfl_sync(FULL, v1, base + 7);
-  ch.hz[2] = __shfl_sync(FULL, v2, base + 0);
+  const int lane = threadIdx.x & (G - 1);
+  const int base = (threadIdx.x & 31) & ~(G - 1);
+  // component j: axis j / 3 (x, y, z), cell offset j % 3 - 1
+  int32_t mine[(9 + G - 1) / G];
+#pragma unroll
+  for (int m = 0; m < (9 + G - 1) / G; m++) {
+    const int j = lane + G * m;
+    const int axis = (j < 9) ? j / 3 : 2;
+    const float pa = (axis == 0) ? px : ((axis == 1) ? py : pz);
+    const double K = (axis == 0) ? 92837111.0 : ((axis == 1) ? 689287499.0 : 283923481.0);
+    const double c = floor(__dmul_rn((double)pa, inv));
+    mine[m] = js_toint32(__dmul_rn(__dadd_rn(c, (double)(j - 3 * axis - 1)), K));
+  }
+  int32_t comp[9];
+#pragma unroll
+  for (int j = 0; j < 9; j++) comp[j] = __shfl_sync(FULL, mine[j / G], base + (j % G));
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    ch.hx[d] = comp[d];
+    ch.hy[d] = comp[3 + d];
+    ch.hz[d] = comp[6 + d];
+  }
 }
 
 // Walk the candidates of the 27 neighbour buckets as ONE sequence: cells in
 // the reference's order k = (dx+1)*9 + (dy+1)*3 + (dz+1), each bucket's PART
 // entries in bucket order (PART 0: its fluid entries, PART 1: its solids);
-// lane l of the GL group takes candidates c = l, l+GL, l+2GL, ... so the
+// lane l of the G group takes candidates c = l, l+G, l+2G, ... so the
 // lanes' shares differ by at most one. For each slot e of its share, in
 // order, a lane calls use(e, load(e)). The bucket ranges are looked up by
-// their round-robin lanes (cell k by lane k mod GL), scanned into sequence
+// their round-robin lanes (cell k by lane k mod G), scanned into sequence
 // offsets by shuffles, and handed over in shared memory. Every lane of the
 // warp must call it; a group with `walk` false has an empty sequence. At most
 // 256 threads per block.
-static __shared__ uint32_t s_walk_base[256 / GL][28];  // slot of candidate 0 of cell k, minus its offset
-static __shared__ uint32_t s_walk_off[256 / GL][28];   // sequence offset of cell k ([27] = total)
+static __shared__ uint32_t s_walk_base[256 / GLF][28];  // slot of candidate 0 of cell k, minus its offset
+static __shared__ uint32_t s_walk_off[256 / GLF][28];   // sequence offset of cell k ([27] = total)
 
-template <int PART, class Load, class Use>
+template <int PART, int G = GL, class Load, class Use>
 __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Load&& load,
                                              Use&& use) {
-  auto& s_base = s_walk_base;  // shared by both parts' instantiations
+  static_assert(G <= GL && GLF <= G, "walk tables are sized for GLF..GL lanes");
+  auto& s_base = s_walk_base;  // shared by every instantiation
   auto& s_off = s_walk_off;
   const unsigned FULL = 0xffffffffu;
   const uint32_t mask = (uint32_t)v.T - 1u;
-  const int g = threadIdx.x / GL;
+  const int g = threadIdx.x / G;
   uint32_t run = 0;
 #pragma unroll
-  for (int m = 0; m < 4; m++) {
-    const int k = lane + GL * m;
+  for (int m = 0; m < (27 + G - 1) / G; m++) {
+    const int k = lane + G * m;
     uint32_t s = 0, n = 0;
     if (walk && k < 27) {
       const uint32_t hb = ch.bucket_k(k, mask);
@@ -251,12 +262,12 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
     }
     uint32_t x = n;  // inclusive scan over the group's lanes (cell order within the round)
 #pragma unroll
-    for (int d = 1; d < GL; d <<= 1) {
-      const uint32_t y = __shfl_up_sync(FULL, x, d, GL);
+    for (int d = 1; d < G; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, x, d, G);
       if (lane >= d) x += y;
     }
     const uint32_t off = run + x - n;
-    run += __shfl_sync(FULL, x, GL - 1, GL);
+    run += __shfl_sync(FULL, x, G - 1, G);
     if (k < 27) {
       s_base[g][k] = s - off;
       s_off[g][k] = off;
@@ -267,7 +278,7 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
   uint32_t k = 0, next = s_off[g][1], base = s_base[g][0];
   // one candidate per step: unrolling to keep several loads in flight cost
   // more in registers (occupancy) than it won in latency on B200
-  for (uint32_t c = (uint32_t)lane; c < run; c += GL) {
+  for (uint32_t c = (uint32_t)lane; c < run; c += G) {
     while (c >= next) {  // next non-empty cell (the total ends the sequence)
       k++;
       next = s_off[g][k + 1];

@@ -203,16 +203,16 @@ __device__ __forceinline__ void b_rankfix(const SimView& v, uint32_t vb) {
 }
 
 // ------------------------------------------------------------------ fluid
-// The neighbour gathers run GL lanes per particle (see lane_strided): a warp
-// holds 32/GL particles, every lane reaches the shuffles, and lane 0 writes.
-// Groups take the particles in slot order (group g: the particle at slot g of
-// this substep's grid, entries[g]): the particles of one bucket sit in
-// consecutive slots and share their 27 neighbour buckets, so a warp's
+// The fluid-fluid gathers run GLF lanes per particle (see lane_strided): a
+// warp holds 32/GLF particles, every lane reaches the shuffles, and lane 0
+// writes. Groups take the particles in slot order (group g: the particle at
+// slot g of this substep's grid, entries[g]): the particles of one bucket sit
+// in consecutive slots and share their 27 neighbour buckets, so a warp's
 // candidate loads mostly hit L1. A particle's own arithmetic does not depend
 // on which group runs it. Groups whose slot holds a solid, or lies past the
 // active count start[T], have no work.
 __device__ __forceinline__ void slot_group(const SimView& v, uint32_t t, uint32_t& e0, uint32_t& i, bool& fluid) {
-  e0 = t / GL;
+  e0 = t / GLF;
   const uint32_t nact = __ldg(&v.start[v.T]);
   i = (e0 < nact) ? v.entries[e0] : 0u;
   fluid = e0 < nact && i >= (uint32_t)v.S;
@@ -222,7 +222,7 @@ __device__ __forceinline__ void slot_group(const SimView& v, uint32_t t, uint32_
 // grid is built from the active particles of this substep, before bounds).
 __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const uint32_t t = UPBD_VTID;
-  const int lane = threadIdx.x & (GL - 1);
+  const int lane = threadIdx.x & (GLF - 1);
   uint32_t myslot, i;
   bool act;
   slot_group(v, t, myslot, i, act);
@@ -230,7 +230,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   float rho = 0.f, rhoNear = 0.f;
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
-  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
+  group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
   const float H = P->fluid_h, H2 = H * H;
   const float4* __restrict__ spos = v.spos;
   // lane l's c-th in-range neighbour goes to row l*NL + c, column myslot
@@ -240,7 +240,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
 #ifndef UPBD_PARITY_BUILD
   const float invH = 1.0f / H;
 #endif
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
+  lane_strided<0, GLF>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
     const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
 #ifdef UPBD_PARITY_BUILD
@@ -263,8 +263,8 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
 #endif
   });
   if (act) v.ncount[lane * NS + myslot] = cnt;
-  rho = lane_sum(rho);
-  rhoNear = lane_sum(rhoNear);
+  rho = lane_sum<GLF>(rho);
+  rhoNear = lane_sum<GLF>(rhoNear);
   if (act && lane == 0) {
     const float2 d = make_float2(rho, rhoNear);
     v.density[i] = d;
@@ -273,8 +273,8 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
 }
 
 // fluidDisp, src/gpu/wgsl.js:281-316, DL threads per slot over the density
-// pass's lists (same positions). Thread h of a slot takes lanes h*GL/DL ..
-// (h+1)*GL/DL - 1: lane l's in-range neighbours in its walk order, then the
+// pass's lists (same positions). Thread h of a slot takes lanes h*GLF/DL ..
+// (h+1)*GLF/DL - 1: lane l's in-range neighbours in its walk order, then the
 // next lane's, summed one after another; the DL partials combine by the xor
 // butterfly. A thread whose lists overflowed walks the 27 buckets for its
 // lanes' shares instead, in the same order. With APPLY it also applies the
@@ -283,7 +283,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
 // read sees a moved particle.
 template <bool APPLY>
 __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
-  constexpr int LPT = GL / DL;  // lanes' lists per thread
+  constexpr int LPT = GLF / DL;  // lanes' lists per thread
   const uint32_t e0 = UPBD_VTID / DL;
   const int h = (int)(threadIdx.x & (DL - 1));
   const uint32_t nact = __ldg(&v.start[v.T]);
@@ -364,7 +364,7 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
         }
       }
     } else {
-      // lane l's share of the walk: candidates c = l, l+GL, ... of the sequence
+      // lane l's share of the walk: candidates c = l, l+GLF, ... of the sequence
       CellHash ch;
       ch.init(pi.x, pi.y, pi.z, P->inv_cell);
       const uint32_t mask = (uint32_t)v.T - 1u;
@@ -374,7 +374,7 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
           const uint32_t hb = ch.bucket_k(kk, mask);
           const uint32_t s0 = __ldg(&v.start[hb]), s1 = __ldg(&v.fend[hb]);
           for (uint32_t e = s0; e < s1; e++, c++)
-            if ((c & (GL - 1)) == (uint32_t)l && e != e0) pair(spos[e], sdens[e]);
+            if ((c & (GLF - 1)) == (uint32_t)l && e != e0) pair(spos[e], sdens[e]);
         }
       }
     }
@@ -992,7 +992,7 @@ __device__ __forceinline__ void b_solid_visc_apply(const SimView& v, uint32_t vb
 template <bool APPLY>
 __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const uint32_t t = UPBD_VTID;
-  const int lane = threadIdx.x & (GL - 1);
+  const int lane = threadIdx.x & (GLF - 1);
   uint32_t myslot, i;
   bool fluid;
   slot_group(v, t, myslot, i, fluid);
@@ -1001,7 +1001,7 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
-  group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
+  group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
   const float H = P->fluid_h, H2 = H * H;
   const float4* __restrict__ spos = v.spos;
   const float4* __restrict__ svel = v.svel;
@@ -1011,16 +1011,16 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   struct PV {
     float4 p, v;
   };
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return PV{spos[e], svel[e]}; }, [&](uint32_t e, const PV& c) {
+  lane_strided<0, GLF>(v, ch, lane, act, [&](uint32_t e) { return PV{spos[e], svel[e]}; }, [&](uint32_t e, const PV& c) {
     const float ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
     const bool in = (e != myslot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
     sx = sx + (in ? c.v.x : 0.f); sy = sy + (in ? c.v.y : 0.f); sz = sz + (in ? c.v.z : 0.f);
     m = m + (in ? 1.0f : 0.f);
   });
-  sx = lane_sum(sx);
-  sy = lane_sum(sy);
-  sz = lane_sum(sz);
-  m = lane_sum(m);
+  sx = lane_sum<GLF>(sx);
+  sy = lane_sum<GLF>(sy);
+  sz = lane_sum<GLF>(sz);
+  m = lane_sum<GLF>(m);
   if (act && lane == 0) {
     const float4 vi = v.vel[i];
     float vx = vi.x, vy = vi.y, vz = vi.z;

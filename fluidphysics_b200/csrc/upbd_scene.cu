@@ -184,8 +184,8 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.svel = cv.take<float4>(v.N);
   L.slot = cv.take<uint32_t>(v.N);
   L.fend = cv.take<uint32_t>(v.T);
-  L.nbr = cv.take<uint32_t>(std::max<size_t>((size_t)v.N * GL * NL, 1));
-  L.ncount = cv.take<uint32_t>(std::max<size_t>((size_t)v.N * GL, 1));
+  L.nbr = cv.take<uint32_t>(std::max<size_t>((size_t)v.N * GLF * NL, 1));
+  L.ncount = cv.take<uint32_t>(std::max<size_t>((size_t)v.N * GLF, 1));
   L.aoth = cv.take<uint32_t>(std::max<size_t>(hs.adj_other.size(), 1));
   L.ascl = cv.take<float>(std::max<size_t>(hs.adj_scale.size(), 1));
   L.ccount = cv.take<uint32_t>(scc ? std::max(v.S, 1) : 1);

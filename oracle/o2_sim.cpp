@@ -35,24 +35,28 @@ static constexpr uint32_t C_K = 40u;  // src/gpu/wgsl.js:25
 // the two agree bit for bit. The candidates of one part (fluid entries, or
 // solid entries) of the 27 neighbour buckets, cells k = (dx+1)*9 + (dy+1)*3 +
 // (dz+1) in order and each bucket's entries in order, form one sequence c =
-// 0, 1, ...; candidate c goes to lane c mod GL (GL = 8), every lane sums from
-// zero, and the eight partials combine as ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)).
-// fluidDisp instead sums the lanes' shares in lane order, DL partial sums of
-// GL/DL lanes each, combined by the same kind of butterfly.
+// 0, 1, ...; candidate c goes to lane c mod L, every lane sums from zero, and
+// the partials combine by an xor butterfly: for the contacts L = GL = 8,
+// ((p0+p4)+(p2+p6)) + ((p1+p5)+(p3+p7)); for fluidDensity and xsph L = GLF =
+// 4, (p0+p2) + (p1+p3). fluidDisp instead sums the GLF lanes' shares in lane
+// order, DL partial sums of GLF/DL lanes each, combined by the same kind of
+// butterfly.
 static constexpr int GL = 8;
+static constexpr int GLF = 4;
 static constexpr int DL = 2;  // fluidDisp threads per particle
 template <class R> static inline R lane_reduce(const R* p) {
   return ((p[0] + p[4]) + (p[2] + p[6])) + ((p[1] + p[5]) + (p[3] + p[7]));
 }
+template <class R> static inline R lane_reduce4(const R* p) { return (p[0] + p[2]) + (p[1] + p[3]); }
 template <class Sim, class V, class Fn>
-static inline void strided_walk(const Sim& s, const V& pi, bool solid_part, Fn&& fn) {
+static inline void strided_walk(const Sim& s, const V& pi, bool solid_part, Fn&& fn, uint32_t lanes = GL) {
   uint32_t c = 0;
   for (int k = 0; k < 27; k++) {
     const uint32_t h = s.cellHashOf(pi, k / 9 - 1, (k / 3) % 3 - 1, k % 3 - 1);
     for (uint32_t e = s.start[h]; e < s.start[h + 1]; e++) {
       const uint32_t j = s.entries[e];
       if ((j < (uint32_t)s.S) != solid_part) continue;
-      fn((int)(c % GL), j);
+      fn((int)(c % lanes), j);
       c++;
     }
   }
@@ -355,7 +359,7 @@ template <class R> void O2Sim<R>::passDensity() {
   for (int i = S; i < N; i++) {
     if (!(flags[i] & F_ACTIVE)) continue;
     const V4<R> pi = pos[i];
-    R rho[GL] = {}, rhoNear[GL] = {};
+    R rho[GLF] = {}, rhoNear[GLF] = {};
     strided_walk(*this, pi, false, [&](int l, uint32_t j) {
       if (j == (uint32_t)i || j < (uint32_t)S) return;
       const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
@@ -364,8 +368,8 @@ template <class R> void O2Sim<R>::passDensity() {
       const R q = LIT(1.0) - std::sqrt(d2) / H;
       rho[l] = rho[l] + q * q;
       rhoNear[l] = rhoNear[l] + q * q * q;
-    });
-    density[i] = V2<R>{lane_reduce(rho), lane_reduce(rhoNear)};
+    }, GLF);
+    density[i] = V2<R>{lane_reduce4(rho), lane_reduce4(rhoNear)};
   }
 }
 
@@ -380,18 +384,18 @@ template <class R> void O2Sim<R>::passDisp() {
     const R Pi = P.stiffness * (density[i].x - P.restDensity);
     const R PNi = P.nearStiffness * density[i].y;
     // DL sums over the neighbours in lane-major order: part h takes lanes
-    // h*GL/DL .. (h+1)*GL/DL - 1, lane l's share of the walk being candidates
-    // c = l, l+GL, ... (the CUDA pass reads them from the density pass's
+    // h*GLF/DL .. (h+1)*GLF/DL - 1, lane l's share of the walk being candidates
+    // c = l, l+GLF, ... (the CUDA pass reads them from the density pass's
     // per-lane lists in that order); the parts combine by the xor butterfly
-    std::vector<uint32_t> share[GL];
+    std::vector<uint32_t> share[GLF];
     strided_walk(*this, pi, false, [&](int l, uint32_t j) {
       if (j != (uint32_t)i && j >= (uint32_t)S) share[l].push_back(j);
-    });
+    }, GLF);
     R part[DL][3] = {};
-    for (int l = 0; l < GL; l++) {
-      R& sx = part[l / (GL / DL)][0];
-      R& sy = part[l / (GL / DL)][1];
-      R& sz = part[l / (GL / DL)][2];
+    for (int l = 0; l < GLF; l++) {
+      R& sx = part[l / (GLF / DL)][0];
+      R& sy = part[l / (GLF / DL)][1];
+      R& sz = part[l / (GLF / DL)][2];
       for (uint32_t j : share[l]) {
         const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
         const R d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -820,15 +824,15 @@ template <class R> void O2Sim<R>::passXsph() {
   for (int i = S; i < N; i++) {
     if (!(flags[i] & F_ACTIVE)) continue;
     const V4<R> pi = pos[i];
-    R qx[GL] = {}, qy[GL] = {}, qz[GL] = {}, qm[GL] = {};
+    R qx[GLF] = {}, qy[GLF] = {}, qz[GLF] = {}, qm[GLF] = {};
     strided_walk(*this, pi, false, [&](int l, uint32_t j) {
       if (j == (uint32_t)i || j < (uint32_t)S) return;
       const R ex = pos[j].x - pi.x, ey = pos[j].y - pi.y, ez = pos[j].z - pi.z;
       if (dot3(ex, ey, ez, ex, ey, ez) >= H2) return;
       qx[l] = qx[l] + vel[j].x; qy[l] = qy[l] + vel[j].y; qz[l] = qz[l] + vel[j].z;
       qm[l] = qm[l] + LIT(1.0);
-    });
-    const R sx = lane_reduce(qx), sy = lane_reduce(qy), sz = lane_reduce(qz), m = lane_reduce(qm);
+    }, GLF);
+    const R sx = lane_reduce4(qx), sy = lane_reduce4(qy), sz = lane_reduce4(qz), m = lane_reduce4(qm);
     R vx = vel[i].x, vy = vel[i].y, vz = vel[i].z;
     if (m > 0) {
       vx = vx + P.viscosity * (sx / m - vx);
