@@ -47,7 +47,15 @@ static constexpr int DL = 2;  // fluidDisp threads per particle
 template <class R> static inline R lane_reduce(const R* p) {
   return ((p[0] + p[4]) + (p[2] + p[6])) + ((p[1] + p[5]) + (p[3] + p[7]));
 }
-template <class R> static inline R lane_reduce4(const R* p) { return (p[0] + p[2]) + (p[1] + p[3]); }
+// the butterfly for any power-of-two lane count G: after the step of width d,
+// lane l holds its value plus lane l+d's (what lane 0 ends with is returned)
+template <int G, class R> static inline R lane_reduce_g(const R* p) {
+  R t[G];
+  for (int l = 0; l < G; l++) t[l] = p[l];
+  for (int d = G / 2; d > 0; d /= 2)
+    for (int l = 0; l < d; l++) t[l] = t[l] + t[l + d];
+  return t[0];
+}
 template <class Sim, class V, class Fn>
 static inline void strided_walk(const Sim& s, const V& pi, bool solid_part, Fn&& fn, uint32_t lanes = GL) {
   uint32_t c = 0;
@@ -369,7 +377,7 @@ template <class R> void O2Sim<R>::passDensity() {
       rho[l] = rho[l] + q * q;
       rhoNear[l] = rhoNear[l] + q * q * q;
     }, GLF);
-    density[i] = V2<R>{lane_reduce4(rho), lane_reduce4(rhoNear)};
+    density[i] = V2<R>{lane_reduce_g<GLF>(rho), lane_reduce_g<GLF>(rhoNear)};
   }
 }
 
@@ -832,7 +840,8 @@ template <class R> void O2Sim<R>::passXsph() {
       qx[l] = qx[l] + vel[j].x; qy[l] = qy[l] + vel[j].y; qz[l] = qz[l] + vel[j].z;
       qm[l] = qm[l] + LIT(1.0);
     }, GLF);
-    const R sx = lane_reduce4(qx), sy = lane_reduce4(qy), sz = lane_reduce4(qz), m = lane_reduce4(qm);
+    const R sx = lane_reduce_g<GLF>(qx), sy = lane_reduce_g<GLF>(qy), sz = lane_reduce_g<GLF>(qz),
+            m = lane_reduce_g<GLF>(qm);
     R vx = vel[i].x, vy = vel[i].y, vz = vel[i].z;
     if (m > 0) {
       vx = vx + P.viscosity * (sx / m - vx);
