@@ -7,6 +7,8 @@ is bit-exact against O2<float> (the WGSL kernels restated) in the
 --fmad=false parity build, and within the stated per-substep tolerance in the
 FMA product build.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -340,21 +342,30 @@ def test_drain_count_reset():
 
 
 def test_graph_and_eager_frames_identical():
+    """Captured graph, eager launches, and the eagerly profiled frame (one
+    stream: the solve's early iterations do not run beside the grid build
+    and the fluid gathers) give the same state bit for bit."""
     sc = S.cpu_scene()
     a = sim_from_scene(sc)
     b = sim_from_scene(sc)
     b.set_graphs(False)
+    c = sim_from_scene(sc)
+    ms = (C.c_double * L.KERNEL_KINDS)()
+    nl = (C.c_uint32 * L.KERNEL_KINDS)()
     o, d1, d2 = S.wedge_through(sc.desc.cube_center, 4)
     for f in range(6):
         if f == 3:
-            a.slice(o, d1, d2)
-            b.slice(o, d1, d2)
+            for s in (a, b, c):
+                s.slice(o, d1, d2)
         a.step(sc.dt, sc.substeps)
         b.step(sc.dt, sc.substeps)
-    sa, sb = a.read_state(), b.read_state()
+        L.check(c.lib, c.h, c.lib.upbd_profile_frame(c.h, sc.dt, sc.substeps, ms, nl))
+    sa, sb, sc_ = a.read_state(), b.read_state(), c.read_state()
     for k in sa:
         assert np.array_equal(sa[k], sb[k]), k
+        assert np.array_equal(sa[k], sc_[k]), k
     assert np.array_equal(a.read_constraints(), b.read_constraints())
+    assert np.array_equal(a.read_constraints(), c.read_constraints())
     assert a.launches > 0
 
 
