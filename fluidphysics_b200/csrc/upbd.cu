@@ -74,7 +74,7 @@ struct upbd_sim {
   // second stream of the substep: the solid solve's first iterations run
   // there beside the grid build and the fluid gathers (fork / join events)
   cudaStream_t side = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaEvent_t fork_ev = nullptr, grid_ev = nullptr, join_ev = nullptr;
   // host copies for reset
   std::vector<float4> init_pos;
   std::vector<uint4> init_cons;
@@ -183,8 +183,11 @@ int launch_substep(upbd_sim* s, int last) {
   // the displacement pass applies the fluid's move itself. The iterations
   // before the last read and write solid positions only (pos, sbuf), which no
   // pass of the grid build or the fluid gathers writes, so they run on the
-  // side stream meanwhile; the last one (slot copies, contact marks) waits
-  // for both. Eager per-kernel timing keeps one stream.
+  // side stream meanwhile; the last one also writes the solids' slot copies,
+  // so it waits for the grid build, and still runs beside density and
+  // displacement (they read fluid slots only); the contact marks, which read
+  // the displaced fluid, follow on the main stream. Eager per-kernel timing
+  // keeps one stream.
   const bool fold = iters >= 2 && !tets && !scc && last >= UPBD_PASS_SOLID;
   const bool overlap = fold && !s->prof_on && s->side;
   const int solid_pad = ((v.S * GL + 31) / 32) * 32;  // lane threads of the solve, whole warps
@@ -196,13 +199,19 @@ int launch_substep(upbd_sim* s, int last) {
       k_solid_solve<false, SOLVE_STEP><<<blocks_for(solid_pad), 256, 0, s->side>>>(v, P, solid_pad, it);
       L++;
     }
-    UPBD_CK(s, cudaEventRecord(s->join_ev, s->side));
   }
   PROF(s, K_SCAN, k_scan<<<v.num_tiles, SCAN_THREADS, 0, st>>>(v));
   PROF(s, K_SCATTER, k_scatter<<<blocks_for(std::max(v.N, tile_words(v.num_tiles))), 256, 0, st>>>(v));
   PROF(s, K_RANKFIX, k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v));
   L += 4;
   UPBD_KCK(s);
+  if (overlap) {
+    UPBD_CK(s, cudaEventRecord(s->grid_ev, st));
+    UPBD_CK(s, cudaStreamWaitEvent(s->side, s->grid_ev, 0));
+    k_solid_solve<false, SOLVE_FINAL><<<blocks_for(solid_pad), 256, 0, s->side>>>(v, P, solid_pad, iters - 1);
+    L++;
+    UPBD_CK(s, cudaEventRecord(s->join_ev, s->side));
+  }
   if (last < UPBD_PASS_DENSITY) return UPBD_OK;
   const long long fl = (long long)v.N * GLF;  // lane-parallel fluid gathers over the slots
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
@@ -230,15 +239,17 @@ int launch_substep(upbd_sim* s, int last) {
   if (fold) {
     if (overlap) {
       UPBD_CK(s, cudaStreamWaitEvent(st, s->join_ev, 0));
+      PROF(s, K_APPLY_SOLID, k_contact_mark<<<blocks_for((long long)v.S * GL), 256, 0, st>>>(v, P));
+      L++;
     } else {
       for (int it = 0; it < iters - 1; it++) {
         PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_STEP><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));
         L++;
       }
+      PROF(s, K_SOLID_SOLVE,
+           k_solid_solve<false, SOLVE_LAST><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, iters - 1));
+      L++;
     }
-    PROF(s, K_SOLID_SOLVE,
-         k_solid_solve<false, SOLVE_LAST><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, iters - 1));
-    L++;
   }
   for (int it = 0; it < iters && !fold; it++) {
     if (it == 0)
@@ -494,6 +505,7 @@ int upbd_create(const upbd_scene_desc* desc, const upbd_params* params, upbd_sim
   s->own_stream = true;
   if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->grid_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess)
     return cleanup_fail(UPBD_ERR_CUDA, "side stream creation failed");
   if (cudaHostAlloc((void**)&s->stage, sizeof(DevParams) * kStageRing, cudaHostAllocDefault) != cudaSuccess)
@@ -548,6 +560,7 @@ int upbd_destroy(upbd_sim* s) {
     cudaStreamDestroy(s->side);
   }
   if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+  if (s->grid_ev) cudaEventDestroy(s->grid_ev);
   if (s->join_ev) cudaEventDestroy(s->join_ev);
   delete s;
   return UPBD_OK;

@@ -449,11 +449,12 @@ __device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParam
 //                inactive solids carried over unchanged.
 //   SOLVE_LAST   applies it into pos and the slot copy, then marks the fluid
 //                near the final position (b_apply_solid<true>'s work).
+//   SOLVE_FINAL  as SOLVE_LAST without the marks (b_contact_mark follows).
 // Every solve reads the previous iteration's positions only, as with the
 // split passes, and pos + omega * delta is the same expression, so the
 // folded iterations give the split ones' results bit for bit; they need at
 // least two iterations (the first may not write what it reads).
-constexpr int SOLVE_DELTA = 0, SOLVE_STEP = 1, SOLVE_LAST = 2;
+constexpr int SOLVE_DELTA = 0, SOLVE_STEP = 1, SOLVE_LAST = 2, SOLVE_FINAL = 3;
 template <bool APPLY_FLUID, int OUT = SOLVE_DELTA>
 __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams* __restrict__ P, int solid_pad, int it,
                                               uint32_t vb) {
@@ -522,7 +523,7 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
     v.pos[i] = p;
     v.spos[v.slot[i]] = p;
   }
-  if (P->use_mark) mark_fluid_near(v, P, act ? p : make_float4(0.f, 0.f, 0.f, 0.f), act, lane);
+  if (OUT == SOLVE_LAST && P->use_mark) mark_fluid_near(v, P, act ? p : make_float4(0.f, 0.f, 0.f, 0.f), act, lane);
 }
 
 // applyDeltaSolid, src/gpu/wgsl.js:361-366. With MARK (last iteration of the
