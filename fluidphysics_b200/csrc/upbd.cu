@@ -239,7 +239,7 @@ int launch_substep(upbd_sim* s, int last) {
   if (fold) {
     if (overlap) {
       UPBD_CK(s, cudaStreamWaitEvent(st, s->join_ev, 0));
-      PROF(s, K_APPLY_SOLID, k_contact_mark<<<blocks_for((long long)v.S * GL), 256, 0, st>>>(v, P));
+      PROF(s, K_APPLY_SOLID, k_contact_mark<32><<<blocks_for((long long)v.S * 32), 256, 0, st>>>(v, P));
       L++;
     } else {
       for (int it = 0; it < iters - 1; it++) {
@@ -274,7 +274,7 @@ int launch_substep(upbd_sim* s, int last) {
     }
   }
   if (!mark_in_apply && v.S > 0) {
-    PROF(s, K_APPLY_SOLID, k_contact_mark<<<blocks_for((long long)v.S * GL), 256, 0, st>>>(v, P));
+    PROF(s, K_APPLY_SOLID, k_contact_mark<32><<<blocks_for((long long)v.S * 32), 256, 0, st>>>(v, P));
     L++;
   }
   UPBD_KCK(s);

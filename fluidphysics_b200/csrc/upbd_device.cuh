@@ -238,7 +238,7 @@ static __shared__ uint32_t s_walk_off[256 / GLF][28];   // sequence offset of ce
 template <int PART, int G = GL, class Load, class Use>
 __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Load&& load,
                                              Use&& use) {
-  static_assert(G <= GL && GLF <= G, "walk tables are sized for GLF..GL lanes");
+  static_assert(G <= 32 && GLF <= G, "walk tables are sized for GLF..32 lanes");
   auto& s_base = s_walk_base;  // shared by every instantiation
   auto& s_off = s_walk_off;
   const unsigned FULL = 0xffffffffu;

@@ -419,15 +419,16 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
 // the contacts pass makes the exact test.
 // Every lane of the warp calls it (the hash is shared by shuffles); only
 // active solids walk.
+template <int G = GL>
 __device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, float4 p,
                                                 bool act, int lane) {
   CellHash ch;
-  group_cell_hash(p.x, p.y, p.z, P->inv_cell, ch);
+  group_cell_hash<G>(p.x, p.y, p.z, P->inv_cell, ch);
   const float rsum = P->solid_radius + P->fluid_radius;
   const float lim2 = rsum * rsum * 1.00001f;
   const float4* __restrict__ sfp = v.sfp;  // the fluid has moved by its displacement
   uint32_t* __restrict__ mark = v.mark;
-  lane_strided<0>(v, ch, lane, act, [&](uint32_t e) { return sfp[e]; }, [&](uint32_t e, const float4& pj) {
+  lane_strided<0, G>(v, ch, lane, act, [&](uint32_t e) { return sfp[e]; }, [&](uint32_t e, const float4& pj) {
     const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
     if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
   });
@@ -555,14 +556,16 @@ __device__ __forceinline__ void b_apply_solid(const SimView& v, const DevParams*
   if (P->use_mark) mark_fluid_near(v, P, p, act, lane);
 }
 
-// Contact marking on its own (when the solve's last position update is not
-// applyDeltaSolid, or there are no solve iterations).
+// Contact marking on its own (when the solve's last position update does not
+// carry it), G lanes per solid. Marks are a set, so the lane count is free:
+// a whole warp per solid makes the 27 bucket lookups one round.
+template <int G = GL>
 __device__ __forceinline__ void b_contact_mark(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   if (!P->use_mark) return;
   const int t = UPBD_VTID;
-  const int i = t / GL;
+  const int i = t / G;
   const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
-  mark_fluid_near(v, P, act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (GL - 1));
+  mark_fluid_near<G>(v, P, act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (G - 1));
 }
 
 // latticeRest, src/gpu/wgsl.js:373-381
