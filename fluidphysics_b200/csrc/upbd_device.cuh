@@ -243,7 +243,10 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
   auto& s_off = s_walk_off;
   const unsigned FULL = 0xffffffffu;
   const uint32_t mask = (uint32_t)v.T - 1u;
-  const int g = threadIdx.x / G;
+  // each warp owns 32/GLF rows, its groups the first 32/G of them: warps of
+  // one block may walk with different G (a 32-lane solid warp beside 8-lane
+  // fluid warps), and rows taken as threadIdx.x / G would then overlap
+  const int g = (int)(threadIdx.x >> 5) * (32 / GLF) + (int)(threadIdx.x & 31) / G;
   uint32_t run = 0;
 #pragma unroll
   for (int m = 0; m < (27 + G - 1) / G; m++) {
