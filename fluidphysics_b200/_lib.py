@@ -158,6 +158,8 @@ _SIGS = [
     ("upbd_grab_move", C.c_int, [_P, _F]),
     ("upbd_release", C.c_int, [_P]),
     ("upbd_read_state", C.c_int, [_P, _F, _F, _F, _F, _U]),
+    ("upbd_read_state_async", C.c_int, [_P, _F, _U]),
+    ("upbd_read_wait", C.c_int, [_P]),
     ("upbd_write_state", C.c_int, [_P, _F, _F, _F, _F, _U]),
     ("upbd_read_constraints", C.c_int, [_P, _U]),
     ("upbd_write_constraints", C.c_int, [_P, _U]),

@@ -75,6 +75,10 @@ struct upbd_sim {
   // there beside the grid build and the fluid gathers (fork / join events)
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, grid_ev = nullptr, join_ev = nullptr;
+  // asynchronous readback: device staging copy, copy stream, events
+  void* rb_stage = nullptr;  // float4 pos[N] then uint32 flags[N]
+  cudaStream_t rb_stream = nullptr;
+  cudaEvent_t rb_ready = nullptr, rb_done = nullptr;
   // host copies for reset
   std::vector<float4> init_pos;
   std::vector<uint4> init_cons;
@@ -559,6 +563,13 @@ int upbd_destroy(upbd_sim* s) {
     cudaStreamSynchronize(s->side);
     cudaStreamDestroy(s->side);
   }
+  if (s->rb_stream) {
+    cudaStreamSynchronize(s->rb_stream);
+    cudaStreamDestroy(s->rb_stream);
+  }
+  if (s->rb_ready) cudaEventDestroy(s->rb_ready);
+  if (s->rb_done) cudaEventDestroy(s->rb_done);
+  if (s->rb_stage) cudaFree(s->rb_stage);
   if (s->fork_ev) cudaEventDestroy(s->fork_ev);
   if (s->grid_ev) cudaEventDestroy(s->grid_ev);
   if (s->join_ev) cudaEventDestroy(s->join_ev);
@@ -908,6 +919,40 @@ int upbd_read_state(upbd_sim* s, float* pos4, float* prev4, float* vel4, float* 
   if (density2) UPBD_CK(s, cudaMemcpyAsync(density2, s->v.density, N * 8, cudaMemcpyDeviceToHost, st));
   if (flags) UPBD_CK(s, cudaMemcpyAsync(flags, s->v.flags, N * 4, cudaMemcpyDeviceToHost, st));
   UPBD_CK(s, cudaStreamSynchronize(st));
+  return UPBD_OK;
+}
+
+int upbd_read_state_async(upbd_sim* s, float* pos4, uint32_t* flags) {
+  if (!s) return UPBD_ERR_INVALID;
+  cudaSetDevice(s->device);
+  const size_t N = (size_t)s->v.N;
+  if (!s->rb_stage) {  // first use: staging copy, copy stream and its events
+    if (!s->rb_stream) UPBD_CK(s, cudaStreamCreateWithFlags(&s->rb_stream, cudaStreamNonBlocking));
+    if (!s->rb_ready) UPBD_CK(s, cudaEventCreateWithFlags(&s->rb_ready, cudaEventDisableTiming));
+    if (!s->rb_done) UPBD_CK(s, cudaEventCreateWithFlags(&s->rb_done, cudaEventDisableTiming));
+    UPBD_CK(s, cudaEventRecord(s->rb_done, s->rb_stream));
+    UPBD_CK(s, cudaMalloc(&s->rb_stage, N * 20));  // last: its presence means all are ready
+  }
+  float4* spos = (float4*)s->rb_stage;
+  uint32_t* sflags = (uint32_t*)(spos + N);
+  cudaStream_t st = s->stream;
+  // the staging copy may still be on its way to the host from the last call
+  UPBD_CK(s, cudaStreamWaitEvent(st, s->rb_done, 0));
+  if (pos4) UPBD_CK(s, cudaMemcpyAsync(spos, s->v.pos, N * 16, cudaMemcpyDeviceToDevice, st));
+  if (flags) UPBD_CK(s, cudaMemcpyAsync(sflags, s->v.flags, N * 4, cudaMemcpyDeviceToDevice, st));
+  UPBD_CK(s, cudaEventRecord(s->rb_ready, st));
+  UPBD_CK(s, cudaStreamWaitEvent(s->rb_stream, s->rb_ready, 0));
+  if (pos4) UPBD_CK(s, cudaMemcpyAsync(pos4, spos, N * 16, cudaMemcpyDeviceToHost, s->rb_stream));
+  if (flags) UPBD_CK(s, cudaMemcpyAsync(flags, sflags, N * 4, cudaMemcpyDeviceToHost, s->rb_stream));
+  UPBD_CK(s, cudaEventRecord(s->rb_done, s->rb_stream));
+  return UPBD_OK;
+}
+
+int upbd_read_wait(upbd_sim* s) {
+  if (!s) return UPBD_ERR_INVALID;
+  if (!s->rb_done) return UPBD_OK;
+  cudaSetDevice(s->device);
+  UPBD_CK(s, cudaEventSynchronize(s->rb_done));
   return UPBD_OK;
 }
 

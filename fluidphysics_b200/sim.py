@@ -169,6 +169,15 @@ class Sim:
                                           L.uptr(flags)))
         return dict(pos=pos, prev=prev, vel=vel, density=dens, flags=flags)
 
+    def read_state_async(self, pos, flags) -> None:
+        """Starts copying positions (float32[total, 4]) and flags (uint32[total])
+        into the given host arrays (pinned for an asynchronous copy) as they
+        stand after the work enqueued so far; read_wait() before using them."""
+        self._ck(self.lib.upbd_read_state_async(self.h, L.fptr(pos), L.uptr(flags)))
+
+    def read_wait(self) -> None:
+        self._ck(self.lib.upbd_read_wait(self.h))
+
     def write_state(self, pos=None, prev=None, vel=None, density=None, flags=None) -> None:
         n = self.info.total
 

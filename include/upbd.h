@@ -262,6 +262,17 @@ int upbd_release(upbd_sim* sim);
 /* GpuSim.readState — src/gpu/sim.js:568-583 (any pointer may be NULL). */
 int upbd_read_state(upbd_sim* sim, float* pos4, float* prev4, float* vel4, float* density2,
                     uint32_t* flags);
+/* GpuSim._readBuffer — src/gpu/sim.js:481-490 (copyBufferToBuffer into a
+ * staging buffer, then mapAsync): the positions and flags as they stand
+ * after the work enqueued so far are copied on the device into a staging
+ * copy, in the simulation's stream order, and from there into pos4[total*4]
+ * and flags[total] (either may be NULL) on a copy stream, so the host copy
+ * overlaps the frames stepped after it. The host buffers must be pinned for
+ * the copy to run asynchronously, and must not be read (or passed to another
+ * readback) before upbd_read_wait returns. */
+int upbd_read_state_async(upbd_sim* sim, float* pos4, uint32_t* flags);
+/* Waits until the readbacks started so far have landed in host memory. */
+int upbd_read_wait(upbd_sim* sim);
 /* Writes the particle state (any pointer may be NULL) — restore's buffer
  * writes, src/gpu/sim.js:526-547. */
 int upbd_write_state(upbd_sim* sim, const float* pos4, const float* prev4, const float* vel4,
