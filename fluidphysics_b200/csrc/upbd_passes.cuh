@@ -415,7 +415,7 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
 
 // ------------------------------------------------------------------ solids
 // Marks the fluid particles within contact range of solid i at position p
-// (GL lanes per solid). The bound is widened by 1e-5 so the set only grows:
+// (G lanes per solid). The bound is widened by 1e-5 so the set only grows:
 // the contacts pass makes the exact test.
 // Every lane of the warp calls it (the hash is shared by shuffles); only
 // active solids walk.
