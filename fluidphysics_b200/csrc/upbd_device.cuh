@@ -108,11 +108,17 @@ struct SimView {
   // [fend[h], start[h+1]) solid.
   uint32_t* fend;
   // Density-pass neighbour lists: lane l (of GLF) of the fluid particle at
-  // slot e records the slots of its in-range fluid neighbours, in its walk
-  // order, at nbr[(l*NL + c) * N + e] (c < NL), and their number in
-  // ncount[l*N + e].
+  // slot e records the slots of its fluid candidates within the list radius
+  // H * (1 + XSKIN), in its walk order, at nbr[(l*NL + c) * N + e] (c < NL),
+  // those within H flagged with NBR_IN, and their number in ncount[l*N + e].
   uint32_t* nbr;
   uint32_t* ncount;
+  // Movement between the density pass and xsph (written by the bounds pass):
+  // smove[e] for the fluid particle at slot e (+inf when it left its cell),
+  // bmove[h] the largest movement above XMOVE_REC * the allowance among the
+  // particles of bucket h (float bits; cleared by the scan).
+  float* smove;
+  uint32_t* bmove;
   const uint32_t* adj_other;  // CSR-parallel: the other endpoint of constraint ids[k]
   const float* adj_scale;     // CSR-parallel: 1 / max(deg_i, deg_other) (static)
   uint32_t* mark;      // per particle: a solid is within contact range (fluid only)
@@ -184,6 +190,23 @@ constexpr int GLF = 4;
 constexpr uint32_t NL = 32;  // density-pass neighbour-list entries kept per fluid lane (GLF * NL per particle)
 constexpr int DL = 2;        // threads per particle in the displacement pass
 
+// xsph sums over the fluid candidates within H at its own time, after the
+// displacement, contact and bounds passes moved the fluid. The density pass
+// lists every candidate within H * (1 + XSKIN), so when the particle kept its
+// cell (the same 27 buckets, the same candidate sequence) and it and every
+// particle of those buckets moved by at most `allowance` = XSKIN * H *
+// XMOVE_FRAC in total, every candidate within H at xsph time is on its lanes'
+// lists, in walk order: xsph reads the lists instead of walking the buckets,
+// and the sums are the walk's sums bit for bit (each lane's skipped candidates
+// would add +0 to sums that start at +0). The rest of the allowance (1 -
+// XMOVE_FRAC) covers the rounding of the distance tests. Movements at or
+// below XMOVE_REC * allowance are not recorded per bucket: a bucket counts
+// them as that much.
+constexpr float XSKIN = 0.05f;
+constexpr float XMOVE_FRAC = 0.9f;
+constexpr float XMOVE_REC = 0.25f;
+constexpr uint32_t NBR_IN = 0x80000000u;  // list entry flag: within H at density time (slots stay below 2^31)
+
 template <int G = GL>
 __device__ __forceinline__ float lane_sum(float x) {
 #pragma unroll
@@ -227,7 +250,8 @@ __device__ __forceinline__ void group_cell_hash(float px, float py, float pz, do
 // entries in bucket order (PART 0: its fluid entries, PART 1: its solids);
 // lane l of the G group takes candidates c = l, l+G, l+2G, ... so the
 // lanes' shares differ by at most one. For each slot e of its share, in
-// order, a lane calls use(e, load(e)). The bucket ranges are looked up by
+// order, a lane calls use(e, load(e)); with U > 1 it issues the loads of U
+// slots before their uses. The bucket ranges are looked up by
 // their round-robin lanes (cell k by lane k mod G), scanned into sequence
 // offsets by shuffles, and handed over in shared memory. Every lane of the
 // warp must call it; a group with `walk` false has an empty sequence. At most
@@ -235,7 +259,7 @@ __device__ __forceinline__ void group_cell_hash(float px, float py, float pz, do
 static __shared__ uint32_t s_walk_base[256 / GLF][28];  // slot of candidate 0 of cell k, minus its offset
 static __shared__ uint32_t s_walk_off[256 / GLF][28];   // sequence offset of cell k ([27] = total)
 
-template <int PART, int G = GL, class Load, class Use>
+template <int PART, int G = GL, int U = 1, class Load, class Use>
 __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Load&& load,
                                              Use&& use) {
   static_assert(G <= 32 && GLF <= G, "walk tables are sized for GLF..32 lanes");
@@ -279,16 +303,45 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
   if (lane == 0) s_off[g][27] = run;
   __syncwarp();
   uint32_t k = 0, next = s_off[g][1], base = s_base[g][0];
-  // one candidate per step: unrolling to keep several loads in flight cost
-  // more in registers (occupancy) than it won in latency on B200
-  for (uint32_t c = (uint32_t)lane; c < run; c += G) {
-    while (c >= next) {  // next non-empty cell (the total ends the sequence)
-      k++;
-      next = s_off[g][k + 1];
-      base = s_base[g][k];
+  if (U == 1) {
+    // one candidate per step: where every group walks, unrolling to keep
+    // several loads in flight costs more in registers (occupancy) than it
+    // wins in latency on B200
+    for (uint32_t c = (uint32_t)lane; c < run; c += G) {
+      while (c >= next) {  // next non-empty cell (the total ends the sequence)
+        k++;
+        next = s_off[g][k + 1];
+        base = s_base[g][k];
+      }
+      const uint32_t e = base + c;
+      use(e, load(e));
     }
-    const uint32_t e = base + c;
-    use(e, load(e));
+  } else {
+    // U candidates per step, their loads in flight together (for the few
+    // groups that walk while the rest of the kernel reads lists)
+    for (uint32_t c0 = (uint32_t)lane; c0 < run; c0 += G * U) {
+      uint32_t e[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const uint32_t c = c0 + (uint32_t)(u * G);
+        if (c < run) {
+          while (c >= next) {
+            k++;
+            next = s_off[g][k + 1];
+            base = s_base[g][k];
+          }
+          e[u] = base + c;
+        } else {
+          e[u] = e[0];  // c0 < run: a valid slot, loaded again and not used
+        }
+      }
+      decltype(load(0u)) x[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) x[u] = load(e[u]);
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        if (c0 + (uint32_t)(u * G) < run) use(e[u], x[u]);
+    }
   }
   __syncwarp();  // the next call may rewrite this group's cells
 }

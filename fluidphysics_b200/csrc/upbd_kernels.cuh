@@ -104,8 +104,10 @@ __global__ void __launch_bounds__(256) k_solid_visc(SimView v, const DevParams* 
   b_solid_visc(v, P, blockIdx.x);
 }
 __global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) { b_solid_visc_apply(v, blockIdx.x); }
-template <bool APPLY>
-__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) { b_xsph<APPLY>(v, P, blockIdx.x); }
+template <bool APPLY, int ROLE = 0>
+__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) {
+  b_xsph<APPLY, ROLE>(v, P, blockIdx.x);
+}
 __global__ void __launch_bounds__(256) k_count_active(SimView v) { b_count_active(v, blockIdx.x, gridDim.x); }
 
 // ------------------------------------------------------------------ tools

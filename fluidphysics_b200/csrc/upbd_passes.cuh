@@ -154,6 +154,10 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
     const uint4 z = make_uint4(0u, 0u, 0u, 0u);  // ready for the next count
     *reinterpret_cast<uint4*>(v.counts + t0) = z;
     *reinterpret_cast<uint4*>(v.counts + t0 + 4) = z;
+    if (v.bmove) {  // no movement recorded yet this substep
+      *reinterpret_cast<uint4*>(v.bmove + t0) = z;
+      *reinterpret_cast<uint4*>(v.bmove + t0 + 4) = z;
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -162,6 +166,7 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
         v.start[idx] = r[k];
         if (v.fend) v.fend[idx] = r[k];
         v.counts[idx] = 0u;
+        if (v.bmove) v.bmove[idx] = 0u;
       }
     }
   }
@@ -232,8 +237,9 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   CellHash ch;
   group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
   const float H = P->fluid_h, H2 = H * H;
+  const float HS = H * (1.0f + XSKIN), HS2 = HS * HS;  // list radius (for xsph)
   const float4* __restrict__ spos = v.spos;
-  // lane l's c-th in-range neighbour goes to row l*NL + c, column myslot
+  // lane l's c-th listed candidate goes to row l*NL + c, column myslot
   const uint32_t NS = (uint32_t)v.N;
   uint32_t* __restrict__ nbr = v.nbr + (size_t)lane * NL * NS + myslot;
   uint32_t cnt = 0;
@@ -245,21 +251,23 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
     const float d2 = dot3(ex, ey, ez, ex, ey, ez);
 #ifdef UPBD_PARITY_BUILD
     if (e == myslot) return;
+    if (d2 >= HS2) return;
+    if (cnt < NL) nbr[cnt * NS] = e | ((d2 < H2) ? NBR_IN : 0u);  // for fluidDisp (same positions) and xsph
+    cnt++;
     if (d2 >= H2) return;
     const float q = 1.0f - sqrtf(d2) / H;
     rho = rho + q * q;
     rhoNear = rhoNear + q * q * q;
-    if (cnt < NL) nbr[cnt * NS] = e;  // for fluidDisp, same positions
-    cnt++;
 #else
     // branch-free: every lane of the warp takes the same path per candidate
     const bool in = (e != myslot) && (d2 < H2);
+    const bool listed = (e != myslot) && (d2 < HS2);
     const float q = 1.0f - approx_sqrt(d2) * invH;
     const float qq = in ? q * q : 0.0f;
     rho = rho + qq;
     rhoNear = rhoNear + qq * q;
-    if (in && cnt < NL) nbr[cnt * NS] = e;  // for fluidDisp, same positions
-    cnt += in ? 1u : 0u;
+    if (listed && cnt < NL) nbr[cnt * NS] = e | (in ? NBR_IN : 0u);  // for fluidDisp (same positions) and xsph
+    cnt += listed ? 1u : 0u;
 #endif
   });
   if (act) v.ncount[lane * NS + myslot] = cnt;
@@ -274,8 +282,8 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
 
 // fluidDisp, src/gpu/wgsl.js:281-316, DL threads per slot over the density
 // pass's lists (same positions). Thread h of a slot takes lanes h*GLF/DL ..
-// (h+1)*GLF/DL - 1: lane l's in-range neighbours in its walk order, then the
-// next lane's, summed one after another; the DL partials combine by the xor
+// (h+1)*GLF/DL - 1: lane l's in-range neighbours (its NBR_IN entries) in its
+// walk order, then the next lane's, summed one after another; the DL partials combine by the xor
 // butterfly. A thread whose lists overflowed walks the 27 buckets for its
 // lanes' shares instead, in the same order. With APPLY it also applies the
 // displacement (applyDeltaFluid, src/gpu/wgsl.js:318-323): pos[i] and the own
@@ -351,8 +359,12 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
           float4 pj[4];
           float2 dj[4];
 #pragma unroll
-          for (int w = 0; w < 4; w++)
-            e[w] = (c + w < cnt[u]) ? __ldg(&nbr[((uint32_t)(l0 + u) * NL + c + w) * NS]) : e0;
+          for (int w = 0; w < 4; w++) {
+            // entries beyond H (listed for xsph) and past the count become the
+            // own slot, which pair() skips (d2 = 0)
+            const uint32_t r = (c + w < cnt[u]) ? __ldg(&nbr[((uint32_t)(l0 + u) * NL + c + w) * NS]) : e0;
+            e[w] = (r & NBR_IN) ? (r & ~NBR_IN) : e0;
+          }
 #pragma unroll
           for (int w = 0; w < 4; w++) {
             pj[w] = spos[e[w]];
@@ -862,6 +874,32 @@ __device__ __forceinline__ void b_bond_contacts(const SimView& v, const DevParam
 }
 
 // -------------------------------- apply + bounds + velocity (per particle)
+// The movement allowance of xsph's list test (XSKIN above), the same float on
+// both sides of the test.
+__device__ __forceinline__ float xsph_allowance(const DevParams* __restrict__ P) {
+  return XSKIN * P->fluid_h * XMOVE_FRAC;
+}
+
+// Records how far fluid particle i (at slot sl) moved since the density pass
+// (o: the position that pass saw, which its slot copy holds until the bounds
+// pass writes p there): smove
+// gets the distance (+inf when the particle left its cell or a coordinate is
+// not finite), and its grid bucket's bmove the largest distance above the
+// recording threshold.
+__device__ __forceinline__ void record_move(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t sl,
+                                            const float4& o, const float4& p) {
+  const float dx = p.x - o.x, dy = p.y - o.y, dz = p.z - o.z;
+  const float INF = __int_as_float(0x7f800000);
+  float m = sqrtf(dot3(dx, dy, dz, dx, dy, dz));
+  if (!(m <= 3.0e38f)) m = INF;  // NaN or inf
+  const double inv = P->inv_cell;
+  const bool same = floor(__dmul_rn((double)o.x, inv)) == floor(__dmul_rn((double)p.x, inv)) &&
+                    floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
+                    floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
+  v.smove[sl] = same ? m : INF;
+  if (m > XMOVE_REC * xsph_allowance(P)) atomicMax(&v.bmove[v.cell[i]], __float_as_uint(m));
+}
+
 // applyDeltaAll (src/gpu/wgsl.js:648-660), bounds (src/gpu/wgsl.js:663-697)
 // and velocityUpdate (src/gpu/wgsl.js:700-710): each touches only its own
 // particle, so one launch runs all three. stage 1/2/3 stops after the first,
@@ -875,6 +913,8 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   const bool iSolid = i < v.S;
   const float r = iSolid ? P->solid_radius : P->fluid_radius;
   float4 p = v.pos[i];
+  const uint32_t sl = v.slot[i];
+  const float4 o = iSolid ? p : v.spos[sl];  // a fluid particle's density-pass position, read before any store
   // applyDeltaAll
   {
     const float4 dd = v.delta[i];
@@ -886,9 +926,9 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
     }
     p.x = p.x + dx; p.y = p.y + dy; p.z = p.z + dz;
   }
-  const uint32_t sl = v.slot[i];
   if (stage < 2) {
     v.pos[i] = p;
+    if (!iSolid) record_move(v, P, i, sl, o, p);
     v.spos[sl] = p;
     return;
   }
@@ -923,6 +963,7 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   }
   p.x = px; p.y = py; p.z = pz;
   v.pos[i] = p;
+  if (!iSolid) record_move(v, P, i, sl, o, p);
   v.spos[sl] = p;
   if (stage < 3) return;
   if (culled) {
@@ -993,7 +1034,16 @@ __device__ __forceinline__ void b_solid_visc_apply(const SimView& v, uint32_t vb
 // APPLY the blended velocity goes straight to vel[i] (xsphApply's result,
 // src/gpu/wgsl.js:773-778) and the copy pass is not needed; without it the
 // result waits in delta, where the reference's xsph pass leaves it.
-template <bool APPLY>
+// A group whose particle passes the list test (XSKIN) reads its lanes'
+// density-pass lists instead of walking the 27 buckets: each lane's listed
+// candidates are a subsequence, in order, of its walk share that holds every
+// candidate within H now, so both forms add the same terms in the same order.
+constexpr int XCH = 4;  // list entries whose loads are in flight together
+constexpr int XWU = 4;  // candidates in flight per step of a walk beside the lists
+// ROLE 0 runs both forms; ROLE 1 only the groups that read lists, ROLE 2
+// only those that walk (two launches that can run side by side: the walking
+// one keeps the walk's register count).
+template <bool APPLY, int ROLE = 0>
 __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GLF - 1);
@@ -1015,17 +1065,62 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   struct PV {
     float4 p, v;
   };
-  lane_strided<0, GLF>(v, ch, lane, act, [&](uint32_t e) { return PV{spos[e], svel[e]}; }, [&](uint32_t e, const PV& c) {
+  auto load = [&](uint32_t e) { return PV{spos[e], svel[e]}; };
+  auto use = [&](uint32_t e, const PV& c) {
     const float ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
     const bool in = (e != myslot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
     sx = sx + (in ? c.v.x : 0.f); sy = sy + (in ? c.v.y : 0.f); sz = sz + (in ? c.v.z : 0.f);
     m = m + (in ? 1.0f : 0.f);
-  });
+  };
+  // the list test: the particle kept its cell (smove finite), it and every
+  // particle of its 27 buckets moved within the allowance, and no lane's list
+  // overflowed
+  const uint32_t NS = (uint32_t)v.N;
+  uint32_t bm = 0, cnt = 0;
+  if (act) {
+    const uint32_t mask = (uint32_t)v.T - 1u;
+#pragma unroll
+    for (int r = 0; r < (27 + GLF - 1) / GLF; r++) {
+      const int k = lane + GLF * r;
+      if (k < 27) bm = max(bm, v.bmove[ch.bucket_k(k, mask)]);
+    }
+    cnt = v.ncount[lane * NS + myslot];
+  }
+  uint32_t over = (cnt > NL) ? 1u : 0u;
+#pragma unroll
+  for (int d = 1; d < GLF; d <<= 1) {
+    bm = max(bm, __shfl_xor_sync(0xffffffffu, bm, d));
+    over |= __shfl_xor_sync(0xffffffffu, over, d);
+  }
+  const float allow = xsph_allowance(P);
+  const float others = fmaxf(XMOVE_REC * allow, __uint_as_float(bm));  // bm holds a finite distance or +inf
+  const bool listed = act && over == 0u && v.smove[myslot] + others <= allow;
+  const bool walks = act && !listed;
+  const bool mine = (ROLE == 0) ? act : ((ROLE == 1) ? listed : walks);
+  if (ROLE != 0 && !__any_sync(0xffffffffu, mine)) return;
+  // with both forms in one launch the groups that walk keep XWU candidates'
+  // loads in flight: while most groups read lists, the few walks are the
+  // kernel's tail
+  if (ROLE != 1 && __any_sync(0xffffffffu, walks)) lane_strided<0, GLF, (ROLE == 0 ? XWU : 1)>(v, ch, lane, walks, load, use);
+  if (ROLE != 2 && listed) {
+    const uint32_t* __restrict__ nbr = v.nbr + (size_t)lane * NL * NS + myslot;
+    for (uint32_t c = 0; c < cnt; c += XCH) {  // XCH entries' loads in flight
+      uint32_t e[XCH];
+      PV pv[XCH];
+#pragma unroll
+      for (int w = 0; w < XCH; w++) e[w] = (c + w < cnt) ? (__ldg(&nbr[(c + w) * NS]) & ~NBR_IN) : myslot;
+#pragma unroll
+      for (int w = 0; w < XCH; w++) pv[w] = load(e[w]);
+#pragma unroll
+      for (int w = 0; w < XCH; w++)
+        if (c + w < cnt) use(e[w], pv[w]);
+    }
+  }
   sx = lane_sum<GLF>(sx);
   sy = lane_sum<GLF>(sy);
   sz = lane_sum<GLF>(sz);
   m = lane_sum<GLF>(m);
-  if (act && lane == 0) {
+  if (mine && lane == 0) {
     const float4 vi = v.vel[i];
     float vx = vi.x, vy = vi.y, vz = vi.z;
     if (m > 0.f) {

@@ -192,6 +192,8 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.clist = cv.take<uint32_t>(scc ? (size_t)std::max(v.S, 1) * C_K : 1);
   L.sbuf = cv.take<float4>(2 * (size_t)std::max(v.S, 1));
   L.sfp = cv.take<float4>(v.N);
+  L.smove = cv.take<float>(v.N);
+  L.bmove = cv.take<uint32_t>(v.T);
   L.scr = cv.take<uint32_t>(SCR_WORDS);
   L.par = cv.take<DevParams>(1);
   L.bytes = cv.off;
@@ -231,6 +233,8 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.clist = (uint32_t*)(base + L.clist);
   v.sbuf = (float4*)(base + L.sbuf);
   v.sfp = (float4*)(base + L.sfp);
+  v.smove = (float*)(base + L.smove);
+  v.bmove = (uint32_t*)(base + L.bmove);
   v.scratch = (uint32_t*)(base + L.scr);
   if (params) *params = (DevParams*)(base + L.par);
 }

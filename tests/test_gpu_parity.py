@@ -245,6 +245,40 @@ def test_frame_parity_build_bit_exact(c1_settled):
     assert np.array_equal(sim.read_constraints(), o2.read_constraints()[0])
 
 
+def test_xsph_lists_and_walks_bit_exact(c2_settled):
+    """xsph reads the density pass's neighbour lists for a particle that kept
+    its cell in a quiet neighbourhood and walks the 27 buckets otherwise. A
+    crowded cluster dropped into the pool (lists past their capacity, large
+    displacements, cell changes) beside the undisturbed fluid makes one
+    substep use both forms, in the one-launch (eager timing) and the split
+    launches; the result matches the oracle bit for bit."""
+    sc, st, cons = c2_settled
+    st = {k: v.copy() for k, v in st.items()}
+    fl = np.flatnonzero(st["flags"][sc.solid_n:] & 1) + sc.solid_n
+    rng = np.random.default_rng(5)
+    pick = rng.choice(fl, 200, replace=False)
+    H = float(sc.params.fluid_h)
+    centre = st["pos"][pick[0], :3].copy()
+    st["pos"][pick, :3] = centre + rng.uniform(-0.3 * H, 0.3 * H, (200, 3)).astype(np.float32)
+    h = sc.dt / sc.substeps
+    o2 = o2_from_scene(sc)
+    o2.write_state(**st)
+    o2.write_constraints(cons)
+    o2.step(h, 1)
+    ref = o2.read_state()
+    ms = (C.c_double * L.KERNEL_KINDS)()
+    nl = (C.c_uint32 * L.KERNEL_KINDS)()
+    for profiled in (False, True):
+        sim = sim_from_scene(sc, "parity")
+        load_state(sim, st, cons)
+        if profiled:  # per-kernel timing: both forms in one xsph launch
+            L.check(sim.lib, sim.h, sim.lib.upbd_profile_frame(sim.h, h, 1, ms, nl))
+        else:
+            sim.step(h, 1)
+        assert_states_equal(sim.read_state(), ref, f"crowded substep (profiled={profiled})")
+        sim.close()
+
+
 @pytest.mark.parametrize("features", [L.FEAT_TETS, L.FEAT_SOLID_CONTACTS,
                                       L.FEAT_TETS | L.FEAT_SOLID_CONTACTS])
 def test_optional_passes_bit_exact(features):
