@@ -45,6 +45,7 @@ constexpr int SCR_CUT = 3;         // constraints cut by the last wedge
 constexpr int SCR_ACTIVE = 4;      // active-fluid partial sums
 constexpr int SCR_DONE = 5;        // blocks finished (last-block pattern)
 constexpr int SCR_HEALTH = 6;      // UPBD_HEALTH_* bits
+constexpr int SCR_XMOVE = 7;       // largest movement the bounds pass recorded this substep (float bits)
 constexpr int SCR_WORDS = 16;
 // mapped host words
 constexpr int HM_ACTIVE = 0;

@@ -171,6 +171,7 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
     }
   }
   if (vb == (uint32_t)v.num_tiles - 1u && tid == SCAN_THREADS - 1) v.start[v.T] = run;
+  if (vb == 0 && tid == 0 && v.bmove) v.scratch[SCR_XMOVE] = 0u;
 }
 
 // Scatter by ticket (gridScatter, src/gpu/wgsl.js:238-245, without its
@@ -882,10 +883,10 @@ __device__ __forceinline__ float xsph_allowance(const DevParams* __restrict__ P)
 
 // Records how far fluid particle i (at slot sl) moved since the density pass
 // (o: the position that pass saw, which its slot copy holds until the bounds
-// pass writes p there): smove
-// gets the distance (+inf when the particle left its cell or a coordinate is
-// not finite), and its grid bucket's bmove the largest distance above the
-// recording threshold.
+// pass writes p there): smove gets the distance (+inf when the particle left
+// its cell or a coordinate is not finite), its grid bucket's bmove and the
+// scene's SCR_XMOVE the largest distance above the recording threshold (the
+// latter one atomic per warp).
 __device__ __forceinline__ void record_move(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t sl,
                                             const float4& o, const float4& p) {
   const float dx = p.x - o.x, dy = p.y - o.y, dz = p.z - o.z;
@@ -897,7 +898,11 @@ __device__ __forceinline__ void record_move(const SimView& v, const DevParams* _
                     floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
                     floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
   v.smove[sl] = same ? m : INF;
-  if (m > XMOVE_REC * xsph_allowance(P)) atomicMax(&v.bmove[v.cell[i]], __float_as_uint(m));
+  const bool rec = m > XMOVE_REC * xsph_allowance(P);
+  if (rec) atomicMax(&v.bmove[v.cell[i]], __float_as_uint(m));
+  const unsigned am = __activemask();
+  const uint32_t wm = __reduce_max_sync(am, rec ? __float_as_uint(m) : 0u);
+  if (wm != 0u && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&v.scratch[SCR_XMOVE], wm);
 }
 
 // applyDeltaAll (src/gpu/wgsl.js:648-660), bounds (src/gpu/wgsl.js:663-697)
@@ -1054,8 +1059,6 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   if (!__any_sync(0xffffffffu, act)) return;
   float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
   const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
-  CellHash ch;
-  group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
   const float H = P->fluid_h, H2 = H * H;
   const float4* __restrict__ spos = v.spos;
   const float4* __restrict__ svel = v.svel;
@@ -1074,27 +1077,36 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   };
   // the list test: the particle kept its cell (smove finite), it and every
   // particle of its 27 buckets moved within the allowance, and no lane's list
-  // overflowed
+  // overflowed. The scene's largest recorded movement bounds every bucket's,
+  // so when it passes the buckets are not looked at (nor hashed, unless the
+  // group walks).
   const uint32_t NS = (uint32_t)v.N;
-  uint32_t bm = 0, cnt = 0;
-  if (act) {
-    const uint32_t mask = (uint32_t)v.T - 1u;
-#pragma unroll
-    for (int r = 0; r < (27 + GLF - 1) / GLF; r++) {
-      const int k = lane + GLF * r;
-      if (k < 27) bm = max(bm, v.bmove[ch.bucket_k(k, mask)]);
-    }
-    cnt = v.ncount[lane * NS + myslot];
-  }
+  const float allow = xsph_allowance(P), rec = XMOVE_REC * allow;
+  const float sm = act ? v.smove[myslot] : 0.f;
+  const uint32_t cnt = act ? v.ncount[lane * NS + myslot] : 0u;
   uint32_t over = (cnt > NL) ? 1u : 0u;
 #pragma unroll
-  for (int d = 1; d < GLF; d <<= 1) {
-    bm = max(bm, __shfl_xor_sync(0xffffffffu, bm, d));
-    over |= __shfl_xor_sync(0xffffffffu, over, d);
+  for (int d = 1; d < GLF; d <<= 1) over |= __shfl_xor_sync(0xffffffffu, over, d);
+  const bool quick = act && over == 0u && sm + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
+  const bool need = act && !quick;  // its buckets' movement, or the walk
+  CellHash ch;
+  bool listed = quick;
+  if (__any_sync(0xffffffffu, need)) {
+    group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
+    uint32_t bm = 0;
+    if (need) {
+      const uint32_t mask = (uint32_t)v.T - 1u;
+#pragma unroll
+      for (int r = 0; r < (27 + GLF - 1) / GLF; r++) {
+        const int k = lane + GLF * r;
+        if (k < 27) bm = max(bm, v.bmove[ch.bucket_k(k, mask)]);
+      }
+    }
+#pragma unroll
+    for (int d = 1; d < GLF; d <<= 1) bm = max(bm, __shfl_xor_sync(0xffffffffu, bm, d));
+    // bm holds a finite distance or +inf
+    listed = quick || (need && over == 0u && sm + fmaxf(rec, __uint_as_float(bm)) <= allow);
   }
-  const float allow = xsph_allowance(P);
-  const float others = fmaxf(XMOVE_REC * allow, __uint_as_float(bm));  // bm holds a finite distance or +inf
-  const bool listed = act && over == 0u && v.smove[myslot] + others <= allow;
   const bool walks = act && !listed;
   const bool mine = (ROLE == 0) ? act : ((ROLE == 1) ? listed : walks);
   if (ROLE != 0 && !__any_sync(0xffffffffu, mine)) return;
