@@ -1043,7 +1043,10 @@ __device__ __forceinline__ void b_solid_visc_apply(const SimView& v, uint32_t vb
 // density-pass lists instead of walking the 27 buckets: each lane's listed
 // candidates are a subsequence, in order, of its walk share that holds every
 // candidate within H now, so both forms add the same terms in the same order.
-constexpr int XCH = 4;  // list entries whose loads are in flight together
+// list entries whose loads are in flight together: 2 in the list-only
+// launch (48 registers: more warps hide the latency), 4 where one launch also
+// walks
+constexpr int XCH_LIST = 2, XCH_BOTH = 4;
 constexpr int XWU = 4;  // candidates in flight per step of a walk beside the lists
 // ROLE 0 runs both forms; ROLE 1 only the groups that read lists, ROLE 2
 // only those that walk (two launches that can run side by side: the walking
@@ -1115,6 +1118,7 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   // kernel's tail
   if (ROLE != 1 && __any_sync(0xffffffffu, walks)) lane_strided<0, GLF, (ROLE == 0 ? XWU : 1)>(v, ch, lane, walks, load, use);
   if (ROLE != 2 && listed) {
+    constexpr int XCH = (ROLE == 1) ? XCH_LIST : XCH_BOTH;
     const uint32_t* __restrict__ nbr = v.nbr + (size_t)lane * NL * NS + myslot;
     for (uint32_t c = 0; c < cnt; c += XCH) {  // XCH entries' loads in flight
       uint32_t e[XCH];
