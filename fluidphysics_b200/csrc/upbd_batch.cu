@@ -75,7 +75,11 @@ __device__ __forceinline__ uint32_t find_scene(const uint32_t* __restrict__ pre,
 // The persistent loop: virtual block vb = blockIdx.x, += gridDim.x, is
 // uniform across the CTA, so pass bodies keep whole warps and may
 // synchronize the CTA (SYNC bodies use shared memory between iterations).
-template <int D, bool SYNC, class Fn>
+// The body sees the scene's SimView as a copy or, with BYREF, in place in
+// the table (its fields loaded where the body uses them): which one needs
+// fewer registers depends on the body, and the kernels below choose by
+// measurement.
+template <int D, bool SYNC, bool BYREF = false, class Fn>
 __device__ __forceinline__ void batch_loop(const BatchArgs& a, Fn&& fn) {
   const uint32_t n = __ldg(a.meta);
   const uint32_t* __restrict__ pre = a.prefix + (size_t)D * a.stride;
@@ -83,8 +87,13 @@ __device__ __forceinline__ void batch_loop(const BatchArgs& a, Fn&& fn) {
   for (uint32_t vb = blockIdx.x; vb < total; vb += gridDim.x) {
     const uint32_t s = find_scene(pre, n, vb);
     const uint32_t b0 = __ldg(pre + s);
-    const SimView v = a.views[s];
-    fn(v, a.params + s, vb - b0, __ldg(pre + s + 1) - b0);
+    if constexpr (BYREF) {
+      const SimView& v = a.views[s];
+      fn(v, a.params + s, vb - b0, __ldg(pre + s + 1) - b0);
+    } else {
+      const SimView v = a.views[s];
+      fn(v, a.params + s, vb - b0, __ldg(pre + s + 1) - b0);
+    }
     if (SYNC) __syncthreads();
   }
 }
@@ -96,19 +105,21 @@ __host__ __device__ __forceinline__ int bond_pad_of(int C, int NT) { return ((C 
 
 template <bool INTEGRATE, bool COUNT>
 __global__ void __launch_bounds__(256) kb_integrate_count(BatchArgs a) {
-  batch_loop<D_N, false>(a, UPBD_BODY { b_integrate_count<INTEGRATE, COUNT>(v, P, vb); });
+  batch_loop<D_N, false, true>(a, UPBD_BODY { b_integrate_count<INTEGRATE, COUNT>(v, P, vb); });
 }
 __global__ void __launch_bounds__(SCAN_THREADS) kb_scan(BatchArgs a) {
-  batch_loop<D_TILES, true>(a, UPBD_BODY { b_scan(v, vb); });
+  batch_loop<D_TILES, true, true>(a, UPBD_BODY { b_scan(v, vb); });
 }
 __global__ void __launch_bounds__(256) kb_scatter(BatchArgs a) {
   batch_loop<D_SCATTER, false>(a, UPBD_BODY { b_scatter(v, vb); });
 }
 __global__ void __launch_bounds__(256) kb_rankfix(BatchArgs a) {
-  batch_loop<D_N, false>(a, UPBD_BODY { b_rankfix(v, vb); });
+  batch_loop<D_N, false, true>(a, UPBD_BODY { b_rankfix(v, vb); });
 }
-__global__ void __launch_bounds__(256) kb_density(BatchArgs a) {
-  batch_loop<D_FGL, false>(a, UPBD_BODY { b_density(v, P, vb); });
+// density and the solve are latency-bound: at most 40 registers (6 CTAs of
+// 256 per SM) hides more of it than the few spilled values cost
+__global__ void __launch_bounds__(256, 6) kb_density(BatchArgs a) {
+  batch_loop<D_FGL, false, true>(a, UPBD_BODY { b_density(v, P, vb); });
 }
 template <bool APPLY>
 __global__ void __launch_bounds__(256) kb_disp(BatchArgs a) {
@@ -118,8 +129,8 @@ __global__ void __launch_bounds__(256) kb_apply_fluid(BatchArgs a) {
   batch_loop<D_F, false>(a, UPBD_BODY { b_apply_fluid(v, vb); });
 }
 template <bool APPLY_FLUID, int OUT>
-__global__ void __launch_bounds__(256) kb_solid_solve(BatchArgs a, int it) {
-  batch_loop<APPLY_FLUID ? D_SOLVE0 : D_SOLVE, false>(
+__global__ void __launch_bounds__(256, 6) kb_solid_solve(BatchArgs a, int it) {
+  batch_loop<APPLY_FLUID ? D_SOLVE0 : D_SOLVE, false, true>(
       a, UPBD_BODY { b_solid_solve<APPLY_FLUID, OUT>(v, P, solid_pad_of(v.S), it, vb); });
 }
 template <bool MARK>
