@@ -260,18 +260,14 @@ __device__ __forceinline__ void group_cell_hash(float px, float py, float pz, do
 static __shared__ uint32_t s_walk_base[256 / GLF][28];  // slot of candidate 0 of cell k, minus its offset
 static __shared__ uint32_t s_walk_off[256 / GLF][28];   // sequence offset of cell k ([27] = total)
 
-template <int PART, int G = GL, int U = 1, class Load, class Use>
-__device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Load&& load,
-                                             Use&& use) {
-  static_assert(G <= 32 && GLF <= G, "walk tables are sized for GLF..32 lanes");
+// The shared tables of a walk: row g (this lane's group) gets the slot base
+// and sequence offset of each of the 27 cells; returns the sequence length.
+template <int PART, int G>
+__device__ __forceinline__ uint32_t walk_tables(const SimView& v, const CellHash& ch, int lane, bool walk, int g) {
   auto& s_base = s_walk_base;  // shared by every instantiation
   auto& s_off = s_walk_off;
   const unsigned FULL = 0xffffffffu;
   const uint32_t mask = (uint32_t)v.T - 1u;
-  // each warp owns 32/GLF rows, its groups the first 32/G of them: warps of
-  // one block may walk with different G (a 32-lane solid warp beside 8-lane
-  // fluid warps), and rows taken as threadIdx.x / G would then overlap
-  const int g = (int)(threadIdx.x >> 5) * (32 / GLF) + (int)(threadIdx.x & 31) / G;
   uint32_t run = 0;
 #pragma unroll
   for (int m = 0; m < (27 + G - 1) / G; m++) {
@@ -303,6 +299,20 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
   }
   if (lane == 0) s_off[g][27] = run;
   __syncwarp();
+  return run;
+}
+
+template <int PART, int G = GL, int U = 1, class Load, class Use>
+__device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& ch, int lane, bool walk, Load&& load,
+                                             Use&& use) {
+  static_assert(G <= 32 && GLF <= G, "walk tables are sized for GLF..32 lanes");
+  auto& s_base = s_walk_base;
+  auto& s_off = s_walk_off;
+  // each warp owns 32/GLF rows, its groups the first 32/G of them: warps of
+  // one block may walk with different G (a 32-lane solid warp beside 8-lane
+  // fluid warps), and rows taken as threadIdx.x / G would then overlap
+  const int g = (int)(threadIdx.x >> 5) * (32 / GLF) + (int)(threadIdx.x & 31) / G;
+  const uint32_t run = walk_tables<PART, G>(v, ch, lane, walk, g);
   uint32_t k = 0, next = s_off[g][1], base = s_base[g][0];
   if (U == 1) {
     // one candidate per step: where every group walks, unrolling to keep
@@ -345,6 +355,53 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
     }
   }
   __syncwarp();  // the next call may rewrite this group's cells
+}
+
+// The same walk for warps where only a few groups walk: for each walking
+// group in turn, all 32 lanes of the warp load its next 32 candidates (one
+// each, all in flight together) into shared memory, and the group's lanes
+// then use them in their own order (lane l: candidates l, l+G, ..., as in
+// lane_strided, so the results are the same bit for bit). Every lane of the
+// warp must call it; at most 256 threads per block.
+template <int PART, int G, class Load, class Use>
+__device__ __forceinline__ void lane_staged(const SimView& v, const CellHash& ch, int lane, bool walk, Load&& load,
+                                            Use&& use) {
+  static_assert(G <= 32 && GLF <= G && 32 % G == 0, "walk tables are sized for GLF..32 lanes");
+  using X = decltype(load(0u));
+  __shared__ X s_x[256 / 32][32];
+  __shared__ uint32_t s_e[256 / 32][32];
+  auto& s_base = s_walk_base;
+  auto& s_off = s_walk_off;
+  const int w = (int)(threadIdx.x >> 5), L = (int)(threadIdx.x & 31);
+  const int g = w * (32 / GLF) + L / G;
+  walk_tables<PART, G>(v, ch, lane, walk, g);
+  unsigned todo = __ballot_sync(0xffffffffu, walk && lane == 0);  // one bit per walking group
+  while (todo) {
+    const int first = __ffs(todo) - 1;  // the group's lane 0
+    todo &= todo - 1u;
+    const int gw = w * (32 / GLF) + first / G;
+    const bool mine = (L / G) == (first / G);
+    const uint32_t run = s_off[gw][27];
+    uint32_t k = 0, next = s_off[gw][1], base = s_base[gw][0];
+    for (uint32_t c0 = 0; c0 < run; c0 += 32) {
+      const uint32_t c = c0 + (uint32_t)L;
+      if (c < run) {
+        while (c >= next) {
+          k++;
+          next = s_off[gw][k + 1];
+          base = s_base[gw][k];
+        }
+        const uint32_t e = base + c;
+        s_e[w][L] = e;
+        s_x[w][L] = load(e);
+      }
+      __syncwarp();
+      if (mine)
+        for (uint32_t j = (uint32_t)lane; j < 32u && c0 + j < run; j += G) use(s_e[w][j], s_x[w][j]);
+      __syncwarp();
+    }
+  }
+  __syncwarp();  // the next call may rewrite this warp's rows
 }
 
 // Square roots inside the gathers' candidate loops. The parity build keeps

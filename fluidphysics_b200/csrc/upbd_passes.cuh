@@ -1116,7 +1116,15 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   // with both forms in one launch the groups that walk keep XWU candidates'
   // loads in flight: while most groups read lists, the few walks are the
   // kernel's tail
-  if (ROLE != 1 && __any_sync(0xffffffffu, walks)) lane_strided<0, GLF, (ROLE == 0 ? XWU : 1)>(v, ch, lane, walks, load, use);
+  if (ROLE == 0 && __any_sync(0xffffffffu, walks)) lane_strided<0, GLF, XWU>(v, ch, lane, walks, load, use);
+  // the walking launch: where one or two groups of a warp walk, the warp's
+  // lanes load their candidates for them; where more do, each walks its own
+  // (staged walks take turns, so they cost more than they save there)
+  if (ROLE == 2) {
+    const unsigned wg = __ballot_sync(0xffffffffu, walks && lane == 0);
+    if (wg != 0u && __popc(wg) <= 2) lane_staged<0, GLF>(v, ch, lane, walks, load, use);
+    else if (wg != 0u) lane_strided<0, GLF, 1>(v, ch, lane, walks, load, use);
+  }
   if (ROLE != 2 && listed) {
     constexpr int XCH = (ROLE == 1) ? XCH_LIST : XCH_BOTH;
     const uint32_t* __restrict__ nbr = v.nbr + (size_t)lane * NL * NS + myslot;
