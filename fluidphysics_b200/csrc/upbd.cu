@@ -313,9 +313,10 @@ int launch_substep(upbd_sim* s, int last) {
   }
   if (!s->prof_on && s->side) {
     // xsph as two launches side by side: the groups that walk on the side
-    // stream, with the walk's own register count (its launch first, so its
-    // long warps start early), and those that read their lists on the main
-    // stream. Eager per-kernel timing keeps the one launch of both forms.
+    // stream (its launch first, so its long warps start early) and those that
+    // read their lists on the main stream, each launch with the registers its
+    // own form needs. Eager per-kernel timing keeps the one launch of both
+    // forms.
     UPBD_CK(s, cudaEventRecord(s->fork_ev, st));
     UPBD_CK(s, cudaStreamWaitEvent(s->side, s->fork_ev, 0));
     k_xsph<true, 2><<<blocks_for((long long)v.N * GLF), 256, 0, s->side>>>(v, P);

@@ -1049,8 +1049,8 @@ __device__ __forceinline__ void b_solid_visc_apply(const SimView& v, uint32_t vb
 constexpr int XCH_LIST = 2, XCH_BOTH = 4;
 constexpr int XWU = 4;  // candidates in flight per step of a walk beside the lists
 // ROLE 0 runs both forms; ROLE 1 only the groups that read lists, ROLE 2
-// only those that walk (two launches that can run side by side: the walking
-// one keeps the walk's register count).
+// only those that walk (two launches that run side by side, each with the
+// registers its own form needs).
 template <bool APPLY, int ROLE = 0>
 __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const uint32_t t = UPBD_VTID;
