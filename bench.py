@@ -247,7 +247,7 @@ def run_reference(args) -> None:
 def run_batched(args, stream, hbm: float) -> dict:
     """The uneven batch: 256 independent scenes (body dim uniform in 6..20,
     fluid log-uniform in [2k, 65k], one seed each) stepped together, one
-    persistent launch per pass; grid shape autotuned first. The state (~5 GB)
+    persistent launch per pass; grid shape autotuned first. The state (~4.3 GB)
     is far larger than L2, so no flush is needed between frames. Beside it,
     the plain per-scene path (one single-scene handle per scene, each frame
     its own captured graph) on a sample of the same scenes."""

@@ -61,3 +61,25 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     args = type("A", (), {"steps": 1, "warmup": 0, "gpus": 2})()
     bench.run_reference(args)  # returns at once, prints nothing
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_line(monkeypatch, capsys):
+    """Rank 0 of the reference arm prints one JSON line with the base
+    contract's keys, its CPU baseline and an e2e block without copies."""
+    import json
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import bench
+    monkeypatch.setenv("RANK", "0")
+    monkeypatch.setenv("WORLD_SIZE", "1")
+    args = type("A", (), {"steps": 1, "warmup": 0, "gpus": 1})()
+    bench.run_reference(args)
+    lines = [l for l in capsys.readouterr().out.splitlines() if l.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "particle-substeps/s" and d["value"] > 0
+    assert d["higher_is_better"] is True and d["steps"] == 1 and d["n_gpus"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
