@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 UPBD_OK = 0
 ERRORS = {
     -1: "UPBD_ERR_INVALID", -2: "UPBD_ERR_OOM", -3: "UPBD_ERR_CUDA", -4: "UPBD_ERR_TIMEOUT",
-    -5: "UPBD_ERR_NAN", -6: "UPBD_ERR_BUSY", -7: "UPBD_ERR_NO_DEVICE", -8: "UPBD_ERR_CAPACITY",
+    -5: "UPBD_ERR_NAN", -6: "UPBD_ERR_BUSY", -7: "UPBD_ERR_NO_DEVICE", -8: "UPBD_ERR_CAPACITY", -9: "UPBD_ERR_INTERNAL",
 }
 F_ACTIVE = 1
 F_GRABBED = 2

@@ -1149,6 +1149,13 @@ struct GridPool {
   } dev[64];
 };
 GridPool g_pool;
+
+// counts[h] = offsets[h+1] - offsets[h] (the scan clears its own counts)
+__global__ void k_counts_from_offsets(const uint32_t* __restrict__ offsets, uint32_t* __restrict__ counts, int T) {
+  const int h = UPBD_TID;
+  if (h < T) counts[h] = offsets[h + 1] - offsets[h];
+}
+
 }  // namespace
 
 int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t table_size, double cell_size,
@@ -1169,15 +1176,19 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
       cudaDeviceSynchronize();
       cudaFree(pd.mem);
       pd.mem = nullptr;
+      pd.n_cap = pd.t_cap = 0;
     }
     const size_t nc = std::max<size_t>((size_t)n, pd.n_cap), tc = std::max<size_t>((size_t)table_size, pd.t_cap);
-    // tile_words() does not decrease with the tile count: the capacity's words cover every smaller table
-    const size_t bytes = (tc + 3 * nc + tile_words((int)((tc + SCAN_TILE - 1) / SCAN_TILE)) + 64) * 4 + sizeof(DevParams);
+    const size_t bytes = grid_scratch_layout(nc, tc, sizeof(DevParams)).words * 4;
     if (cudaMalloc(&pd.mem, bytes) != cudaSuccess) return fail(nullptr, UPBD_ERR_OOM, "grid scratch allocation failed");
-    if (cudaMemset(pd.mem, 0, bytes) != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, "grid scratch clear failed");
+    // cleared in the caller's stream order: the count kernel below runs on
+    // that stream, which may be a non-blocking one
+    if (cudaMemsetAsync(pd.mem, 0, bytes, st) != cudaSuccess)
+      return fail(nullptr, UPBD_ERR_CUDA, "grid scratch clear failed");
     pd.n_cap = nc;
     pd.t_cap = tc;
   }
+  const GridScratchLayout lay = grid_scratch_layout(pd.n_cap, pd.t_cap, sizeof(DevParams));
   uint32_t* w = (uint32_t*)pd.mem;
   SimView v{};
   v.pos = (float4*)pos4;
@@ -1185,15 +1196,18 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
   v.N = n;
   v.T = table_size;
   v.num_tiles = tiles;
-  v.counts = w;
-  v.ticket = w + pd.t_cap;
-  v.cell = v.ticket + pd.n_cap;
-  v.tmp = v.cell + pd.n_cap;
-  v.tile_sum = v.tmp + pd.n_cap;
+  v.counts = w + lay.counts;
+  v.ticket = w + lay.ticket;
+  v.cell = w + lay.cell;
+  v.tmp = w + lay.tmp;
+  v.tile_sum = w + lay.tiles;
   v.start = (uint32_t*)offsets;
   v.entries = (uint32_t*)entries;
-  // the count kernel reads 1/cell_size from a params block at the pool's tail
-  DevParams* dp = (DevParams*)(v.tile_sum + tile_words((int)((pd.t_cap + SCAN_TILE - 1) / SCAN_TILE)) + 64);
+  // the count kernel reads 1/cell_size (a double) from a params block at the
+  // pool's tail, on a 256-byte boundary
+  DevParams* dp = (DevParams*)(w + lay.params);
+  if ((reinterpret_cast<uintptr_t>(dp) & 15u) != 0)
+    return fail(nullptr, UPBD_ERR_INTERNAL, "grid scratch params block is not 16-byte aligned");
   DevParams hp{};
   hp.inv_cell = 1.0 / cell_size;
   if (cudaMemcpyAsync(dp, &hp, sizeof(DevParams), cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -1202,20 +1216,10 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
   k_scan<<<tiles, SCAN_THREADS, 0, st>>>(v);
   k_scatter<<<blocks_for(std::max(n, tile_words(tiles))), 256, 0, st>>>(v);
   k_rankfix<<<blocks_for(n), 256, 0, st>>>(v);
+  // counts[h] = offsets[h+1] - offsets[h] (the scan cleared its own counts)
+  if (counts) k_counts_from_offsets<<<blocks_for(table_size), 256, 0, st>>>(v.start, (uint32_t*)counts, table_size);
   cudaError_t e = cudaPeekAtLastError();
   if (e != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, cudaGetErrorString(e));
-  if (counts) {
-    // counts[h] = offsets[h+1] - offsets[h] (the scan cleared its own counts)
-    std::vector<uint32_t> off((size_t)table_size + 1);
-    if (cudaMemcpyAsync(off.data(), offsets, off.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return fail(nullptr, UPBD_ERR_CUDA, "offset readback failed");
-    std::vector<uint32_t> c((size_t)table_size);
-    for (int h = 0; h < table_size; h++) c[h] = off[h + 1] - off[h];
-    if (cudaMemcpyAsync(counts, c.data(), c.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return fail(nullptr, UPBD_ERR_CUDA, "count upload failed");
-  }
   return UPBD_OK;
 }
 
@@ -1264,15 +1268,10 @@ namespace {
 
 constexpr int kNoAllocMaxN = 1 << 18;  // particles per call
 constexpr int kNoAllocMaxT = 1 << 18;  // hash buckets per call
-constexpr size_t kNoAllocTiles = (kNoAllocMaxT + SCAN_TILE - 1) / SCAN_TILE;
-// word offsets inside the array
-constexpr size_t kNaCounts = 0;
-constexpr size_t kNaTicket = kNaCounts + kNoAllocMaxT;
-constexpr size_t kNaCell = kNaTicket + kNoAllocMaxN;
-constexpr size_t kNaTmp = kNaCell + kNoAllocMaxN;
-constexpr size_t kNaTiles = kNaTmp + kNoAllocMaxN;
-constexpr size_t kNaParams = ((kNaTiles + tile_words((int)kNoAllocTiles) + 63) / 64) * 64;  // 256-byte aligned
-constexpr size_t kNaWords = kNaParams + (sizeof(DevParams) + 3) / 4;
+// word offsets inside the array (params on a 256-byte boundary)
+constexpr GridScratchLayout kNa = grid_scratch_layout(kNoAllocMaxN, kNoAllocMaxT, sizeof(DevParams));
+static_assert(kNa.params % 64 == 0, "params block must start on a 256-byte boundary");
+constexpr size_t kNaWords = kNa.words;
 
 __device__ __align__(256) uint32_t g_grid_scratch[kNaWords];
 
@@ -1282,12 +1281,6 @@ uint32_t* g_noalloc_ptr[64] = {};  // device address of g_grid_scratch, per devi
 // The hash reads 1/cell_size from a params block: set it on the device from
 // a kernel argument (no host-to-device copy, no staging buffer).
 __global__ void k_noalloc_params(DevParams* p, double inv_cell) { p->inv_cell = inv_cell; }
-
-// counts[h] = offsets[h+1] - offsets[h] (the scan clears its own counts)
-__global__ void k_counts_from_offsets(const uint32_t* __restrict__ offsets, uint32_t* __restrict__ counts, int T) {
-  const int h = UPBD_TID;
-  if (h < T) counts[h] = offsets[h + 1] - offsets[h];
-}
 
 }  // namespace
 
@@ -1328,14 +1321,14 @@ extern "C" int upbd_grid_build_noalloc(const void* pos4, const void* flags, int3
   v.N = n;
   v.T = table_size;
   v.num_tiles = tiles;
-  v.counts = w + kNaCounts;
-  v.ticket = w + kNaTicket;
-  v.cell = w + kNaCell;
-  v.tmp = w + kNaTmp;
-  v.tile_sum = w + kNaTiles;
+  v.counts = w + kNa.counts;
+  v.ticket = w + kNa.ticket;
+  v.cell = w + kNa.cell;
+  v.tmp = w + kNa.tmp;
+  v.tile_sum = w + kNa.tiles;
   v.start = (uint32_t*)offsets;
   v.entries = (uint32_t*)entries;
-  DevParams* dp = (DevParams*)(w + kNaParams);
+  DevParams* dp = (DevParams*)(w + kNa.params);
   // the array keeps the previous call's contents: counts and tile totals
   // must start at zero
   cudaError_t e = cudaMemsetAsync(v.counts, 0, (size_t)table_size * 4, st);

@@ -16,27 +16,14 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "upbd_grid_layout.h"
+
 namespace upbd {
 
 constexpr uint32_t F_ACTIVE = 1u;
 constexpr uint32_t F_GRABBED = 2u;
 constexpr uint32_t C_K = 40u;           // solid contact cache width, src/gpu/wgsl.js:25
-constexpr int SCAN_TILE = 2048;         // counts scanned per block
-constexpr int SCAN_THREADS = 256;       // 8 counts per thread
-
-// The count pass adds every arrival to its scan tile's total. With 2^18
-// buckets there are only 128 tiles, so one counter per tile took ~600 atomics
-// at one L2 address per substep and the kernel's drain dominated its time.
-// Each tile therefore has `tile_reps` counters, a warp adding to counter
-// (warp index mod reps): tile_sum[r * num_tiles + t]. The scan sums them back;
-// reps * num_tiles stays <= 2048 words up to 2^22 buckets, so that sum is at
-// most 8 independent loads per scan thread.
-__host__ __device__ constexpr int tile_reps(int num_tiles) {
-  int r = 16;
-  while (r > 1 && r * num_tiles > 2048) r >>= 1;
-  return r;
-}
-__host__ __device__ constexpr int tile_words(int num_tiles) { return tile_reps(num_tiles) * num_tiles; }
+constexpr int SCAN_THREADS = 256;       // 8 counts per thread (SCAN_TILE / 8)
 
 // scratch words (device)
 constexpr int SCR_PICK_T = 0;      // uint64 bits of the best t (words 0-1)

@@ -58,6 +58,7 @@ extern "C" {
 #define UPBD_ERR_BUSY       -6  /* resource in use (e.g. server full) */
 #define UPBD_ERR_NO_DEVICE  -7  /* no CUDA device / wrong architecture */
 #define UPBD_ERR_CAPACITY   -8  /* request exceeds a fixed capacity */
+#define UPBD_ERR_INTERNAL   -9  /* an internal invariant does not hold (a library bug) */
 
 /* ---- particle flags (src/gpu/wgsl.js:33-34) ---- */
 #define UPBD_F_ACTIVE  1u
@@ -330,8 +331,15 @@ int upbd_groups(upbd_sim* sim, int32_t* group);
  * scatter of src/gpu/wgsl.js:163-245 with Solver._buildGrid's membership
  * order (src/solver.js:174-184). pos4: float4[n] device, flags: uint32[n]
  * device (bit0 = active), counts[T], offsets[T+1], entries[n] device
- * outputs. Scratch comes from a per-device pool allocated on first use.
- * stream = cudaStream_t (NULL = default stream). */
+ * outputs (counts may be NULL). stream = cudaStream_t (NULL = default
+ * stream). Scratch comes from one per-device pool that the library allocates
+ * on first use and grows when a call needs more: growing it calls
+ * cudaDeviceSynchronize, cudaFree and cudaMalloc, so a call that grows the
+ * pool must not be captured into a CUDA graph (make one call of the largest
+ * size first). Every call on a device shares that pool: calls whose work
+ * overlaps on the GPU (different streams or threads) race on it, so order
+ * them on one stream or with events. All work, including the counts, is
+ * enqueued on `stream`; the call does not wait for it. */
 int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t table_size,
                     double cell_size, void* counts, void* offsets, void* entries,
                     void* stream);
@@ -351,7 +359,9 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
  * before any stream capture. Every call shares the one array: calls whose
  * work overlaps on the GPU (other streams, other threads) race and corrupt
  * each other's results, so order them on one stream or with events. Each call
- * clears the parts of the array that must start at zero. */
+ * clears the parts of the array that must start at zero. The device address
+ * is looked up once per device and kept: after cudaDeviceReset on a device,
+ * unload and reload the library before calling this entry point there again. */
 int upbd_grid_build_noalloc(const void* pos4, const void* flags, int32_t n, int32_t table_size,
                             double cell_size, void* counts, void* offsets, void* entries,
                             void* stream);

@@ -12,8 +12,9 @@ input state is produced by the C++ restatement O1 (30 frames of settling) so
 that contacts, plasticity and the pair cap are exercised — its output is
 still produced by the reference code.
 
-Run from the repository root (needs /root/reference):
-    python tests/golden/make_golden.py
+Run from the repository root, naming the reference checkout (its directory
+holding src/solver.js) with --ref or the UPBD_REFERENCE environment variable:
+    python tests/golden/make_golden.py --ref <path to the reference>
 Writes tests/golden/solver_js.json (digests and small arrays) and
 tests/golden/solver_js_c1.npz (full C1 arrays).
 """
@@ -35,7 +36,24 @@ sys.path.insert(0, str(ROOT))
 
 import jsmini as J  # noqa: E402
 
-REF = Path("/root/reference")
+
+
+def _reference_dir() -> Path:
+    import os
+    args = sys.argv[1:]
+    if "--ref" in args and args.index("--ref") + 1 < len(args):
+        ref = args[args.index("--ref") + 1]
+    else:
+        ref = os.environ.get("UPBD_REFERENCE", "")
+    if not ref:
+        raise SystemExit("name the reference checkout: --ref <dir> or UPBD_REFERENCE=<dir>")
+    d = Path(ref)
+    if not (d / "src" / "solver.js").exists():
+        raise SystemExit(f"{d} does not hold src/solver.js")
+    return d
+
+
+REF = _reference_dir() if __name__ == "__main__" else Path(".")
 
 
 def digest(a: np.ndarray) -> str:

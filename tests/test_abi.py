@@ -38,11 +38,30 @@ def test_library_exports_every_declared_symbol(built_libs, variant):
     assert set(L.EXPORTED) == declared_symbols()
 
 
-def test_library_is_sm100a(built_libs):
-    # the fatbin carries sm_100a code only; cuobjdump is not needed for this:
-    # the build flags are the contract
-    from fluidphysics_b200 import build as B
-    assert B.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+def test_grid_scratch_layout_alignment(tmp_path):
+    """The stateless grid builds carve bucket counts, tickets, cells, the
+    scatter, the scan tile counters and a params block (which holds a double)
+    from one base. For every particle count, odd ones included, the params
+    block starts on a 256-byte boundary and the regions do not overlap."""
+    src = tmp_path / "lay.cpp"
+    src.write_text(
+        '#include <cstdio>\n#include "upbd_grid_layout.h"\nusing namespace upbd;\n'
+        "int main(){ const size_t ns[] = {1, 2, 3, 2943, 73535, 73536, 262143, 262144};\n"
+        " const size_t ts[] = {1, 1024, 8192, 262144, 1u << 20};\n"
+        " for (size_t n : ns) for (size_t t : ts) { GridScratchLayout L = grid_scratch_layout(n, t, 304);\n"
+        "  size_t tiles = (t + SCAN_TILE - 1) / SCAN_TILE;\n"
+        "  printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %d\\n\", n, t, L.counts, L.ticket, L.cell, L.tmp, L.tiles,"
+        " L.params, L.words, tile_words((int)tiles)); }\n return 0; }\n")
+    exe = tmp_path / "lay"
+    subprocess.run(["g++", "-std=c++17", "-I", str(ROOT / "fluidphysics_b200" / "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    rows = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    rows = [list(map(int, r.split())) for r in rows if r.strip()]
+    assert len(rows) == 40
+    for n, t, counts, ticket, cell, tmp, tiles, params, words, tw in rows:
+        assert counts == 0 and ticket == t and cell == ticket + n and tmp == cell + n and tiles == tmp + n
+        assert params >= tiles + tw and params % 64 == 0, (n, t)  # 256-byte boundary (double inside)
+        assert words == params + 304 // 4
 
 
 def test_struct_layouts_match_c(tmp_path):

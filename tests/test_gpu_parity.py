@@ -121,6 +121,56 @@ def test_stateless_grid_build_matches():
         assert np.array_equal(d_cnt.cpu().numpy().view(np.uint32), np.diff(cs))
 
 
+_ODD_N_CHILD = r"""
+import ctypes as C, sys
+import numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from fluidphysics_b200 import _lib as L, scenes as S
+from oracle.oracle import o1_from_scene
+sc = S.cpu_scene()
+o1 = o1_from_scene(sc)
+pos = o1.get("pos").reshape(-1, 3)
+act = o1.get("active")
+n, T = pos.shape[0], sc.desc.table_size
+assert n % 2 == 1, n
+p4 = np.zeros((n, 4), np.float32)
+p4[:, :3] = pos
+lib = L.load()
+side = torch.cuda.Stream()  # a non-blocking stream: the scratch clear must be ordered on it
+with torch.cuda.stream(side):
+    d_pos = torch.from_numpy(p4).cuda()
+    d_flags = torch.from_numpy(act.astype(np.int32)).cuda()
+    d_off = torch.full((T + 1,), -1, dtype=torch.int32, device="cuda")
+    d_ent = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    d_cnt = torch.full((T,), -1, dtype=torch.int32, device="cuda")
+    rc = lib.upbd_grid_build(C.c_void_p(d_pos.data_ptr()), C.c_void_p(d_flags.data_ptr()), n, T,
+                             sc.params.cell_size, C.c_void_p(d_cnt.data_ptr()), C.c_void_p(d_off.data_ptr()),
+                             C.c_void_p(d_ent.data_ptr()), C.c_void_p(side.cuda_stream))
+    assert rc == 0, lib.upbd_last_error(None)
+side.synchronize()
+o1.run_pass("grid")
+cs = o1.get("cellStart").astype(np.uint32)
+ce = o1.get("cellEntries").astype(np.uint32)
+assert np.array_equal(d_off.cpu().numpy().view(np.uint32), cs)
+assert np.array_equal(d_ent.cpu().numpy().view(np.uint32)[: cs[-1]], ce[: cs[-1]])
+assert np.array_equal(d_cnt.cpu().numpy().view(np.uint32), np.diff(cs))
+print("odd-n grid ok", n)
+"""
+
+
+def test_stateless_grid_build_odd_n_fresh_process():
+    """The first call of a process sizes the scratch pool: with an odd
+    particle count (2,943) the params block must still be aligned, and the
+    pool's clear must be ordered on the caller's non-blocking stream."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    r = subprocess.run([sys.executable, "-c", _ODD_N_CHILD, str(root)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "odd-n grid ok 2943" in r.stdout
+
+
 # ------------------------------------------------------------------ cut / pick
 def wedges(center, n, seed):
     return [S.wedge_through(np.asarray(center) + np.random.default_rng(seed + k).normal(size=3) * 0.1,

@@ -21,13 +21,14 @@ from fluidphysics_b200 import scenes as S
 pytestmark = pytest.mark.gpu
 
 
-def _grid(torch, lib, fn, pos, flags, n, T, cell):
+def _grid(torch, lib, fn, pos, flags, n, T, cell, with_counts=True):
     dev = pos.device
     off = torch.full((T + 1,), -1, dtype=torch.int32, device=dev)
     ent = torch.full((max(n, 1),), -1, dtype=torch.int32, device=dev)
     cnt = torch.full((T,), -1, dtype=torch.int32, device=dev)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    rc = fn(C.c_void_p(pos.data_ptr()), C.c_void_p(flags.data_ptr()), n, T, cell, C.c_void_p(cnt.data_ptr()),
+    rc = fn(C.c_void_p(pos.data_ptr()), C.c_void_p(flags.data_ptr()), n, T, cell,
+            C.c_void_p(cnt.data_ptr()) if with_counts else None,
             C.c_void_p(off.data_ptr()), C.c_void_p(ent.data_ptr()), stream)
     assert rc == 0, lib.upbd_last_error(None)
     torch.cuda.synchronize()
@@ -63,6 +64,10 @@ def test_noalloc_grid_matches_pooled_build_twice():
         for a, b, what in zip(got, ref, ("offsets", "entries", "counts")):
             assert np.array_equal(a, b), f"{what} differ (n={n}, T={T})"
         assert got[0][-1] == int(flags.sum().item())
+        # counts are optional: without them the offsets and members are the same
+        off, ent, cnt = _grid(torch, lib, lib.upbd_grid_build_noalloc, pos, flags, n, T, cell, with_counts=False)
+        assert np.array_equal(off, ref[0]) and np.array_equal(ent, ref[1])
+        assert (cnt.view(np.int32) == -1).all(), "counts written although none were asked for"
 
 
 def test_noalloc_rejects_sizes_beyond_its_array():
