@@ -47,6 +47,7 @@ def load():
         "o2_create": (P, [P, P, I]), "o2_destroy": (None, [P]), "o2_info": (None, [P, P]),
         "o2_set_params": (None, [P, P]), "o2_step": (None, [P, C.c_double, I]), "o2_frame": (None, [P]),
         "o2_substep_partial": (None, [P, C.c_double, I]), "o2_rebuild_grid": (None, [P]),
+        "o2_run_pass": (I, [P, I, C.c_double]),
         "o2_set_iters": (None, [P, I]),
         "o2_read_state": (None, [P, D, D, D, D, U]), "o2_write_state": (None, [P, D, D, D, D, U]),
         "o2_read_delta": (None, [P, D]), "o2_read_constraints": (None, [P, U, D]),
@@ -206,6 +207,11 @@ class O2:
 
     def rebuild_grid(self) -> None:
         self.lib.o2_rebuild_grid(self.h)
+
+    def run_pass(self, pass_id: int, h: float = 1 / 300) -> None:
+        """One pass (UPBD_PASS_* id) on the current state."""
+        if self.lib.o2_run_pass(self.h, pass_id, h) != 0:
+            raise ValueError(f"pass {pass_id} cannot run alone")
 
     def read_state(self) -> dict:
         n = self.info.total

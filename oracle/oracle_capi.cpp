@@ -194,6 +194,30 @@ void o2_substep_partial(void* h, double hh, int last) {
   DISPATCH(h, { S_.substep((decltype(S_.P.h))hh, last); });
 }
 void o2_rebuild_grid(void* h) { DISPATCH(h, S_.passGrid()); }
+// One pass (UPBD_PASS_* id) on the current state with substep length hh, for
+// pass-by-pass comparisons with O1: GRID, DENSITY, DISP (the displacement
+// into delta), APPLY_FLUID, CONTACTS (into delta), APPLY_ALL, BOUNDS,
+// VELOCITY, XSPH (into delta), XSPH_APPLY. Returns 0, or -1 for another id.
+int o2_run_pass(void* h, int pass, double hh) {
+  int rc = 0;
+  DISPATCH(h, {
+    S_.P.h = (decltype(S_.P.h))hh;
+    switch (pass) {
+      case UPBD_PASS_GRID: S_.passGrid(); break;
+      case UPBD_PASS_DENSITY: S_.passDensity(); break;
+      case UPBD_PASS_DISP: S_.passDisp(); break;
+      case UPBD_PASS_APPLY_FLUID: S_.passApplyFluid(); break;
+      case UPBD_PASS_CONTACTS: S_.passContacts(); break;
+      case UPBD_PASS_APPLY_ALL: S_.passApplyAll(); break;
+      case UPBD_PASS_BOUNDS: S_.passBounds(); break;
+      case UPBD_PASS_VELOCITY: S_.passVelocity(); break;
+      case UPBD_PASS_XSPH: S_.passXsph(); break;
+      case UPBD_PASS_XSPH_APPLY: S_.passXsphApply(); break;
+      default: rc = -1;
+    }
+  });
+  return rc;
+}
 void o2_set_iters(void* h, int iters) { DISPATCH(h, S_.iters = iters); }
 
 void o2_read_state(void* h, double* pos4, double* prev4, double* vel4, double* dens2,
