@@ -33,6 +33,10 @@ constexpr int SCR_ACTIVE = 4;      // active-fluid partial sums
 constexpr int SCR_DONE = 5;        // blocks finished (last-block pattern)
 constexpr int SCR_HEALTH = 6;      // UPBD_HEALTH_* bits
 constexpr int SCR_XMOVE = 7;       // largest movement the bounds pass recorded this substep (float bits)
+constexpr int SCR_REBUILD = 8;     // product build: this substep's density pass rebuilds every fluid list
+constexpr int SCR_DIRTY = 9;       // product build: the lists no longer describe the state (set by tools, culls)
+constexpr int SCR_WALKERS = 10;    // product build: particles that walked the buckets this substep
+constexpr int SCR_REBUILDS = 11;   // product build: substeps that rebuilt the lists (wraps at 2^32)
 constexpr int SCR_WORDS = 16;
 // mapped host words
 constexpr int HM_ACTIVE = 0;
@@ -55,7 +59,10 @@ struct DevParams {
   // 1 when solid_radius + fluid_radius is below the cell size: every
   // solid↔fluid contact then lies in adjacent cells, so the solids can mark
   // the fluid particles that have one and the rest skip their gather.
-  int32_t use_mark, pad4;
+  int32_t use_mark;
+  // 1 when the fluid gathers may keep neighbour lists across substeps
+  // (fluid_h at most the cell size; product build only)
+  int32_t use_lists;
   float4 grab_delta;  // per-substep share of the frame's grab motion
   uint32_t emit_count, emit_start, grab_lattice, pad3;
   float4 emit_pos, emit_dir, emit_side, emit_up;
@@ -117,6 +124,16 @@ struct SimView {
   float4* sfp;
   uint32_t* ccount;
   uint32_t* clist;
+  // Product build: fluid neighbour lists kept across substeps (particle
+  // indices; lane l of fluid particle f = i - S keeps its entries at
+  // nbr[(l*NL + c) * F + f] and their number at ncount[l*F + f], reusing the
+  // parity build's per-substep list arrays), the position each list was
+  // built at (xlist[f]), per-particle state bits (pfl, PF_* below) and a
+  // particle-indexed copy of the velocities for xsph (ivel; w = 1 when the
+  // particle changed cell after the grid build).
+  float4* xlist;
+  uint32_t* pfl;
+  float4* ivel;
   uint32_t* scratch;
   uint32_t* host_mapped;
   int S, N1, dim1, dim2, F, N, C, NT, T, num_tiles;
@@ -165,6 +182,31 @@ struct CellHash {
   }
 };
 
+// True when two of the 27 cells around the cell of CellHash ch share a hash
+// bucket. Cells (a,b,c) and (a',b',c') collide exactly when
+// (X_a^X_a') ^ (Y_b^Y_b') ^ (Z_c^Z_c') is 0 under the mask, so the test runs
+// over the 4 x 4 x 4 choices of equal (0) or one of three pair differences
+// per axis, all but the all-equal one.
+__device__ __forceinline__ bool buckets_coincide(const CellHash& ch, uint32_t mask) {
+  const uint32_t dx[4] = {0u, (uint32_t)(ch.hx[0] ^ ch.hx[1]) & mask, (uint32_t)(ch.hx[0] ^ ch.hx[2]) & mask,
+                          (uint32_t)(ch.hx[1] ^ ch.hx[2]) & mask};
+  const uint32_t dy[4] = {0u, (uint32_t)(ch.hy[0] ^ ch.hy[1]) & mask, (uint32_t)(ch.hy[0] ^ ch.hy[2]) & mask,
+                          (uint32_t)(ch.hy[1] ^ ch.hy[2]) & mask};
+  const uint32_t dz[4] = {0u, (uint32_t)(ch.hz[0] ^ ch.hz[1]) & mask, (uint32_t)(ch.hz[0] ^ ch.hz[2]) & mask,
+                          (uint32_t)(ch.hz[1] ^ ch.hz[2]) & mask};
+  bool hit = false;
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const uint32_t xy = dx[a] ^ dy[b];
+#pragma unroll
+      for (int c = 0; c < 4; c++)
+        if (a | b | c) hit |= (xy == dz[c]);
+    }
+  return hit;
+}
+
 // Neighbour gathers run G lanes per particle (lane_strided below deals the
 // candidates to the lanes); each lane accumulates its own partial sums from
 // zero and the G partials are combined by a fixed xor butterfly, so the
@@ -177,6 +219,14 @@ constexpr int GL = 8;
 constexpr int GLF = 4;
 constexpr uint32_t NL = 32;  // density-pass neighbour-list entries kept per fluid lane (GLF * NL per particle)
 constexpr int DL = 2;        // threads per particle in the displacement pass
+// threads per grid slot of the displacement launch: the parity build's DL
+// threads over the density pass's per-substep lists, the product build's GLF
+// lanes over its lane lists
+#ifdef UPBD_PARITY_BUILD
+constexpr int DISP_LANES = DL;
+#else
+constexpr int DISP_LANES = GLF;
+#endif
 
 // xsph sums over the fluid candidates within H at its own time, after the
 // displacement, contact and bounds passes moved the fluid. The density pass
@@ -194,6 +244,27 @@ constexpr float XSKIN = 0.05f;
 constexpr float XMOVE_FRAC = 0.9f;
 constexpr float XMOVE_REC = 0.25f;
 constexpr uint32_t NBR_IN = 0x80000000u;  // list entry flag: within H at density time (slots stay below 2^31)
+
+// Product build: neighbour lists kept across substeps (Verlet lists). At a
+// rebuild the density pass lists, per lane, every fluid candidate of its walk
+// within H * (1 + VSKIN) and records the particle's position. A later
+// substep may read the list instead of walking the 27 buckets when the
+// particle's own movement since the rebuild plus the largest movement of any
+// particle that can be within H of it stays within VMOVE_FRAC of the skin
+// (the rest covers rounding): then every fluid particle within H is listed.
+// Movements at or below VMOVE_REC * the allowance are not recorded per
+// bucket: a bucket counts them as that much.
+constexpr float VSKIN = 0.25f;
+constexpr float VMOVE_FRAC = 0.9f;
+constexpr float VMOVE_REC = 0.25f;
+// pfl bits
+constexpr uint32_t PF_DUP = 1u;    // two of the 27 buckets around the grid-time cell coincide
+constexpr uint32_t PF_DUPF = 2u;   // the same for the cell at xsph time
+constexpr uint32_t PF_LOK = 4u;    // the list is complete (no lane overflowed, no coinciding buckets at the rebuild)
+constexpr uint32_t PF_LIST = 8u;   // this substep's density and displacement read the list
+// A rebuild follows a substep whose density and xsph passes walked for more
+// than F / VWALK_DIV particles.
+constexpr uint32_t VWALK_DIV = 512u;
 
 template <int G = GL>
 __device__ __forceinline__ float lane_sum(float x) {

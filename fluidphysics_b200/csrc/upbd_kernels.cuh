@@ -13,6 +13,9 @@ namespace upbd {
 __global__ void __launch_bounds__(64) k_emit(SimView v, const DevParams* __restrict__ P) {
   const uint32_t k = UPBD_TID;
   if (k >= P->emit_count) return;
+#ifndef UPBD_PARITY_BUILD
+  if (k == 0) v.scratch[SCR_DIRTY] = 1u;  // new particles: the fluid lists are rebuilt
+#endif
   const int slot = v.S + (int)((P->emit_start + k) % (uint32_t)v.F);
   const float4 E_pos = P->emit_pos, E_dir = P->emit_dir, E_side = P->emit_side, E_up = P->emit_up;
   const float phase = E_dir.w + (float)k * 2.39996f;
@@ -60,13 +63,25 @@ __global__ void __launch_bounds__(256) k_integrate_count(SimView v, const DevPar
 }
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(SimView v) { b_scan(v, blockIdx.x); }
 __global__ void __launch_bounds__(256) k_scatter(SimView v) { b_scatter(v, blockIdx.x); }
-__global__ void __launch_bounds__(256) k_rankfix(SimView v) { b_rankfix(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_rankfix(SimView v, const DevParams* __restrict__ P) {
+  b_rankfix(v, P, blockIdx.x);
+}
+// The fluid gathers: the bucket walks in the parity build (the oracle's
+// summation order), lists kept across substeps in the product build.
 __global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __restrict__ P) {
+#ifdef UPBD_PARITY_BUILD
   b_density(v, P, blockIdx.x);
+#else
+  b_density_vl(v, P, blockIdx.x);
+#endif
 }
 template <bool APPLY>
 __global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __restrict__ P) {
+#ifdef UPBD_PARITY_BUILD
   b_disp<APPLY>(v, P, blockIdx.x);
+#else
+  b_disp_vl<APPLY>(v, P, blockIdx.x);
+#endif
 }
 __global__ void __launch_bounds__(256) k_apply_fluid(SimView v) { b_apply_fluid(v, blockIdx.x); }
 template <bool APPLY_FLUID, int OUT>
@@ -106,7 +121,11 @@ __global__ void __launch_bounds__(256) k_solid_visc(SimView v, const DevParams* 
 __global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) { b_solid_visc_apply(v, blockIdx.x); }
 template <bool APPLY, int ROLE = 0>
 __global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) {
+#ifdef UPBD_PARITY_BUILD
   b_xsph<APPLY, ROLE>(v, P, blockIdx.x);
+#else
+  b_xsph_vl<APPLY>(v, P, blockIdx.x);
+#endif
 }
 __global__ void __launch_bounds__(256) k_count_active(SimView v) { b_count_active(v, blockIdx.x, gridDim.x); }
 

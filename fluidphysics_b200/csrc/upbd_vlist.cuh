@@ -1,0 +1,394 @@
+// Product-build fluid gathers over neighbour lists kept across substeps
+// (Verlet lists): fluidDensity, fluidDisp and xsph of src/gpu/wgsl.js
+// (254-279, 281-323, 745-778) with the same pair sets as the 27-bucket walks
+// and their own summation order (the parity build keeps the walk order of
+// upbd_passes.cuh and matches the oracle bit for bit; this build stays within
+// the stated per-substep tolerance of it).
+//
+// Which pairs the reference counts. Its gathers visit the members of the 27
+// hash buckets around a particle's cell, so particle j enters i's sum once
+// per occurrence of j's bucket among i's 27 buckets, when within H. With no
+// two of those 27 buckets equal (PF_DUP / PF_DUPF clear) and every pair
+// within H in adjacent cells (fluid_h at most the cell size), that is: every
+// fluid j within H, once. xsph runs after the fluid moved but on the grid
+// built before: j counts when its grid-time bucket is among the 27 buckets
+// of i's current cell; for a j that kept its cell since the grid build that
+// holds whenever j is within H, and the others (ivel[j].w = 1) are checked
+// against the 27 buckets explicitly.
+//
+// When lists are complete. A rebuild (density pass, SCR_REBUILD) lists for
+// each lane every fluid candidate of its walk share within H * (1 + VSKIN)
+// and records the position. A list may be read when the particle's movement
+// since then, plus the largest movement of any particle that can be within H
+// of it, stays within the allowance VMOVE_FRAC * VSKIN * H: the scene-wide
+// largest recorded movement settles most particles; otherwise the largest
+// movement recorded in its 27 buckets does (every particle the reference
+// could count sits in one of them). Particles that fail walk the buckets
+// (without touching their lists). A rebuild follows a substep where more
+// than F / VWALK_DIV particles walked, and any change the lists cannot
+// follow (emit, drain, a state write, a cull: SCR_DIRTY).
+#pragma once
+#include "upbd_device.cuh"
+
+namespace upbd {
+
+__device__ __forceinline__ float vl_allowance(const DevParams* __restrict__ P) {
+  return VSKIN * P->fluid_h * VMOVE_FRAC;
+}
+
+__device__ __forceinline__ float vl_dist(const float4& a, const float4& b) {
+  const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  const float m = sqrtf(dot3(dx, dy, dz, dx, dy, dz));
+  return (m <= 3.0e38f) ? m : __int_as_float(0x7f800000);  // NaN / inf -> +inf
+}
+
+// Largest recorded movement (float bits) in the 27 buckets of ch, reduced
+// over the GLF lanes of each group. Every lane of the warp calls it.
+__device__ __forceinline__ uint32_t vl_bucket_move(const SimView& v, const CellHash& ch, bool need, int lane) {
+  uint32_t bm = 0;
+  if (need) {
+    const uint32_t mask = (uint32_t)v.T - 1u;
+#pragma unroll
+    for (int r = 0; r < (27 + GLF - 1) / GLF; r++) {
+      const int k = lane + GLF * r;
+      if (k < 27) bm = max(bm, __ldg(&v.bmove[ch.bucket_k(k, mask)]));
+    }
+  }
+#pragma unroll
+  for (int d = 1; d < GLF; d <<= 1) bm = max(bm, __shfl_xor_sync(0xffffffffu, bm, d));
+  return bm;
+}
+
+// Walkers of this warp's groups (lane 0 of each) into the scene's counter.
+__device__ __forceinline__ void vl_count_walkers(const SimView& v, bool walks, int lane) {
+  const unsigned b = __ballot_sync(0xffffffffu, walks && lane == 0);
+  if (b != 0u && (threadIdx.x & 31) == 0) atomicAdd(&v.scratch[SCR_WALKERS], (uint32_t)__popc(b));
+}
+
+// fluidDensity (src/gpu/wgsl.js:254-279); at a rebuild also writes the lists.
+__device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
+  const unsigned FULL = 0xffffffffu;
+  const bool rebuild = v.scratch[SCR_REBUILD] != 0u;  // one value for the whole scene
+  if (rebuild && vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
+  const uint32_t t = UPBD_VTID;
+  const int lane = threadIdx.x & (GLF - 1);
+  uint32_t myslot, i;
+  bool act;
+  slot_group(v, t, myslot, i, act);
+  if (!__any_sync(FULL, act)) return;
+  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t FS = (uint32_t)v.F;
+  const uint32_t f = act ? i - (uint32_t)v.S : 0u;
+  const uint32_t pf = act ? v.pfl[i] : 0u;
+  const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
+  const float allow = vl_allowance(P), rec = VMOVE_REC * allow;
+  const bool cand = act && !rebuild && P->use_lists && (pf & (PF_LOK | PF_DUP)) == PF_LOK;
+  const float mv = cand ? vl_dist(pi, v.xlist[f]) : 0.f;
+  const bool quick = cand && mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
+  const bool need = cand && !quick && mv + rec <= allow;
+  bool listed = quick;
+  CellHash ch;
+  if (__any_sync(FULL, act && !quick)) {
+    group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
+    const uint32_t bm = vl_bucket_move(v, ch, need, lane);
+    listed = quick || (need && mv + fmaxf(rec, __uint_as_float(bm)) <= allow);
+  }
+  const bool walks = act && !listed;
+  float rho = 0.f, rhoNear = 0.f;
+  uint32_t over = 0u;
+  if (__any_sync(FULL, walks)) {
+    const float HS = H * (1.0f + VSKIN), HS2 = HS * HS;
+    uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
+    const float4* __restrict__ spos = v.spos;
+    uint32_t cnt = 0;
+    lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
+      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      const bool in = (e != myslot) && (d2 < H2);
+      const float q = 1.0f - approx_sqrt(d2) * invH;
+      const float qq = in ? q * q : 0.0f;
+      rho = rho + qq;
+      rhoNear = rhoNear + qq * q;
+      if (rebuild) {
+        const bool keep = (e != myslot) && (d2 < HS2);
+        if (keep && cnt < NL) lst[cnt * FS] = __ldg(&v.entries[e]);
+        cnt += keep ? 1u : 0u;
+      }
+    });
+    if (rebuild && walks) v.ncount[lane * FS + f] = cnt;
+    over = (cnt > NL) ? 1u : 0u;
+#pragma unroll
+    for (int d = 1; d < GLF; d <<= 1) over |= __shfl_xor_sync(FULL, over, d);
+  }
+  if (listed) {
+    const uint32_t n = v.ncount[lane * FS + f];
+    const uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
+    const float4* __restrict__ pos = v.pos;
+    for (uint32_t c = 0; c < n; c += 2) {  // two entries' loads in flight
+      const uint32_t j0 = __ldg(&lst[c * FS]);
+      const uint32_t j1 = (c + 1 < n) ? __ldg(&lst[(c + 1) * FS]) : j0;
+      const float4 p0 = pos[j0], p1 = pos[j1];
+      float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
+      float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      float q = 1.0f - approx_sqrt(d2) * invH;
+      float qq = (d2 < H2) ? q * q : 0.0f;
+      rho = rho + qq;
+      rhoNear = rhoNear + qq * q;
+      ex = p1.x - pi.x; ey = p1.y - pi.y; ez = p1.z - pi.z;
+      d2 = dot3(ex, ey, ez, ex, ey, ez);
+      q = 1.0f - approx_sqrt(d2) * invH;
+      qq = (d2 < H2 && c + 1 < n) ? q * q : 0.0f;
+      rho = rho + qq;
+      rhoNear = rhoNear + qq * q;
+    }
+  }
+  rho = lane_sum<GLF>(rho);
+  rhoNear = lane_sum<GLF>(rhoNear);
+  if (!rebuild) vl_count_walkers(v, walks, lane);
+  if (act && lane == 0) {
+    const float2 d = make_float2(rho, rhoNear);
+    v.density[i] = d;
+    v.sdens[myslot] = d;
+    uint32_t npf = pf;
+    if (rebuild) {
+      v.xlist[f] = pi;
+      npf = (over || (pf & PF_DUP)) ? (npf & ~PF_LOK) : (npf | PF_LOK);
+    }
+    npf = listed ? (npf | PF_LIST) : (npf & ~PF_LIST);
+    v.pfl[i] = npf;
+  }
+}
+
+// fluidDisp (src/gpu/wgsl.js:281-316) over the same pairs as the density
+// pass; with APPLY also applyDeltaFluid (src/gpu/wgsl.js:318-323) into the
+// particle's slot copy sfp (pos[i] is left for the bounds pass to write, so
+// the list reads of pos stay on the pre-displacement positions).
+template <bool APPLY>
+__device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
+  const unsigned FULL = 0xffffffffu;
+  const uint32_t t = UPBD_VTID;
+  const int lane = threadIdx.x & (GLF - 1);
+  uint32_t myslot, i;
+  bool act;
+  slot_group(v, t, myslot, i, act);
+  if (!__any_sync(FULL, act)) return;
+  const bool listed = act && (v.pfl[i] & PF_LIST);
+  const bool walks = act && !listed;
+  const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
+  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float2 di = act ? v.sdens[myslot] : make_float2(0.f, 0.f);
+  const float maxPair = 0.05f * H;
+  const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
+  const float Pi = k * (di.x - rho0);
+  const float PNi = kn * di.y;
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+  auto pair = [&](const float4& pj, const float2& dj) {
+    const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+    if (d2 >= H2 || d2 < 1e-12f) return;
+    const float rd = rsqrtf(d2);
+    const float q = 1.0f - d2 * rd * invH;
+    const float Pj = k * (dj.x - rho0);
+    const float PNj = kn * dj.y;
+    float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
+    D = clampf(D, -maxPair, maxPair);
+    const float f = D * rd;
+    sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
+  };
+  if (__any_sync(FULL, walks)) {
+    CellHash ch;
+    group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
+    struct PD {
+      float4 p;
+      float2 d;
+    };
+    const float4* __restrict__ spos = v.spos;
+    const float2* __restrict__ sdens = v.sdens;
+    lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return PD{spos[e], sdens[e]}; },
+                         [&](uint32_t e, const PD& c) {
+                           if (e != myslot) pair(c.p, c.d);
+                         });
+  }
+  if (listed) {
+    const uint32_t FS = (uint32_t)v.F;
+    const uint32_t f = i - (uint32_t)v.S;
+    const uint32_t n = v.ncount[lane * FS + f];
+    const uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
+    const float4* __restrict__ pos = v.pos;
+    const float2* __restrict__ dens = v.density;
+    for (uint32_t c = 0; c < n; c += 2) {  // two entries' loads in flight
+      const uint32_t j0 = __ldg(&lst[c * FS]);
+      const uint32_t j1 = (c + 1 < n) ? __ldg(&lst[(c + 1) * FS]) : j0;
+      const float4 p0 = pos[j0], p1 = pos[j1];
+      const float2 d0 = dens[j0], d1 = dens[j1];
+      pair(p0, d0);
+      if (c + 1 < n) pair(p1, d1);
+    }
+  }
+#pragma unroll
+  for (int d = 1; d < GLF; d <<= 1) {
+    sx = sx + __shfl_xor_sync(FULL, sx, d);
+    sy = sy + __shfl_xor_sync(FULL, sy, d);
+    sz = sz + __shfl_xor_sync(FULL, sz, d);
+  }
+  if (!act || lane != 0) return;
+  const float maxTotal = 0.35f * H;
+  const float s2 = dot3(sx, sy, sz, sx, sy, sz);
+  if (s2 > maxTotal * maxTotal) {
+    const float f = maxTotal / sqrtf(s2);
+    sx = sx * f; sy = sy * f; sz = sz * f;
+  }
+  if (APPLY)
+    v.sfp[myslot] = make_float4(pi.x + sx, pi.y + sy, pi.z + sz, pi.w);
+  else
+    v.delta[i] = make_float4(sx, sy, sz, 1.0f);
+}
+
+// Records, for the xsph pass, how far fluid particle i (at slot sl) has moved
+// since its list was built (smove, and above VMOVE_REC * the allowance its
+// grid bucket's bmove and the scene's SCR_XMOVE), and whether its final cell
+// differs from its grid-time cell o (returned; then PF_DUPF is tested for the
+// new cell). Called by the bounds pass for every active fluid particle.
+__device__ __forceinline__ bool vl_record(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t sl,
+                                          const float4& o, const float4& p) {
+  const unsigned am = __activemask();  // the lanes that reach the warp reduction below
+  const float m = vl_dist(p, v.xlist[i - v.S]);
+  v.smove[sl] = m;
+  const bool rec = m > VMOVE_REC * vl_allowance(P);
+  if (rec) atomicMax(&v.bmove[v.cell[i]], __float_as_uint(m));
+  const uint32_t wm = __reduce_max_sync(am, rec ? __float_as_uint(m) : 0u);
+  if (wm != 0u && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&v.scratch[SCR_XMOVE], wm);
+  const double inv = P->inv_cell;
+  const bool same = floor(__dmul_rn((double)o.x, inv)) == floor(__dmul_rn((double)p.x, inv)) &&
+                    floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
+                    floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
+  const uint32_t pf = v.pfl[i];
+  bool dupf = (pf & PF_DUP) != 0u;
+  if (!same) {
+    CellHash ch;
+    ch.init(p.x, p.y, p.z, inv);
+    dupf = buckets_coincide(ch, (uint32_t)v.T - 1u);
+  }
+  v.pfl[i] = dupf ? (pf | PF_DUPF) : (pf & ~PF_DUPF);
+  return !same;
+}
+
+// Grid-time movement since the list build, recorded by the rank fix-up for
+// the density pass's test (skipped at a rebuild: the lists are rebuilt from
+// the positions the density pass sees).
+__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h) {
+  const unsigned am = __activemask();  // the lanes that reach the warp reduction below
+  const float m = vl_dist(v.pos[i], v.xlist[i - v.S]);
+  const bool rec = m > VMOVE_REC * vl_allowance(P);
+  if (rec) atomicMax(&v.bmove[h], __float_as_uint(m));
+  const uint32_t wm = __reduce_max_sync(am, rec ? __float_as_uint(m) : 0u);
+  if (wm != 0u && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&v.scratch[SCR_XMOVE], wm);
+}
+
+// j's grid-time bucket is one of the 27 around the cell of p.
+static __device__ __noinline__ bool vl_member(const SimView& v, const DevParams* __restrict__ P, const float4& p,
+                                              uint32_t j) {
+  CellHash ch;
+  ch.init(p.x, p.y, p.z, P->inv_cell);
+  const uint32_t mask = (uint32_t)v.T - 1u, h = v.cell[j];
+  bool hit = false;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) hit |= (ch.bucket(a, b, c, mask) == h);
+  return hit;
+}
+
+// xsph (src/gpu/wgsl.js:745-771) at the final positions; with APPLY the
+// blended velocity goes to vel[i] (xsphApply, src/gpu/wgsl.js:773-778), the
+// neighbours' velocities being read from the copies the velocity pass wrote
+// (svel by slot for walks, ivel by index for lists).
+template <bool APPLY>
+__device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
+  const unsigned FULL = 0xffffffffu;
+  const uint32_t t = UPBD_VTID;
+  const int lane = threadIdx.x & (GLF - 1);
+  uint32_t myslot, i;
+  bool fluid;
+  slot_group(v, t, myslot, i, fluid);
+  const bool act = fluid && (v.flags[i] & F_ACTIVE);
+  if (!__any_sync(FULL, act)) return;
+  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float H = P->fluid_h, H2 = H * H;
+  const float allow = vl_allowance(P), rec = VMOVE_REC * allow;
+  const uint32_t pf = act ? v.pfl[i] : 0u;
+  const float mv = act ? v.smove[myslot] : 0.f;
+  const bool cand = act && P->use_lists && (pf & (PF_LOK | PF_DUPF)) == PF_LOK && mv + rec <= allow;
+  const bool quick = cand && mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
+  const bool need = cand && !quick;
+  bool listed = quick;
+  CellHash ch;
+  if (__any_sync(FULL, act && !quick)) {
+    group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
+    const uint32_t bm = vl_bucket_move(v, ch, need, lane);
+    listed = quick || (need && mv + fmaxf(rec, __uint_as_float(bm)) <= allow);
+  }
+  const bool walks = act && !listed;
+  float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
+  if (__any_sync(FULL, walks)) {
+    struct PV {
+      float4 p, v;
+    };
+    const float4* __restrict__ spos = v.spos;
+    const float4* __restrict__ svel = v.svel;
+    lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return PV{spos[e], svel[e]}; },
+                         [&](uint32_t e, const PV& c) {
+                           const float ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
+                           const bool in = (e != myslot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
+                           sx = sx + (in ? c.v.x : 0.f); sy = sy + (in ? c.v.y : 0.f);
+                           sz = sz + (in ? c.v.z : 0.f); m = m + (in ? 1.0f : 0.f);
+                         });
+  }
+  if (listed) {
+    const uint32_t FS = (uint32_t)v.F;
+    const uint32_t f = i - (uint32_t)v.S;
+    const uint32_t n = v.ncount[lane * FS + f];
+    const uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
+    const float4* __restrict__ pos = v.pos;
+    const float4* __restrict__ ivel = v.ivel;
+    for (uint32_t c = 0; c < n; c += 2) {  // two entries' loads in flight
+      const uint32_t j0 = __ldg(&lst[c * FS]);
+      const uint32_t j1 = (c + 1 < n) ? __ldg(&lst[(c + 1) * FS]) : j0;
+      const float4 p0 = pos[j0], p1 = pos[j1];
+      const float4 u0 = ivel[j0], u1 = ivel[j1];
+      float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
+      bool in = dot3(ex, ey, ez, ex, ey, ez) < H2;
+      if (in && u0.w != 0.f) in = vl_member(v, P, pi, j0);  // j0 changed cell after the grid build
+      sx = sx + (in ? u0.x : 0.f); sy = sy + (in ? u0.y : 0.f); sz = sz + (in ? u0.z : 0.f);
+      m = m + (in ? 1.0f : 0.f);
+      ex = p1.x - pi.x; ey = p1.y - pi.y; ez = p1.z - pi.z;
+      in = (c + 1 < n) && dot3(ex, ey, ez, ex, ey, ez) < H2;
+      if (in && u1.w != 0.f) in = vl_member(v, P, pi, j1);
+      sx = sx + (in ? u1.x : 0.f); sy = sy + (in ? u1.y : 0.f); sz = sz + (in ? u1.z : 0.f);
+      m = m + (in ? 1.0f : 0.f);
+    }
+  }
+  sx = lane_sum<GLF>(sx);
+  sy = lane_sum<GLF>(sy);
+  sz = lane_sum<GLF>(sz);
+  m = lane_sum<GLF>(m);
+  vl_count_walkers(v, walks, lane);
+  if (act && lane == 0) {
+    const float4 vi = v.vel[i];
+    float vx = vi.x, vy = vi.y, vz = vi.z;
+    if (m > 0.f) {
+      const float mu = P->viscosity;
+      vx = vx + mu * (sx / m - vx);
+      vy = vy + mu * (sy / m - vy);
+      vz = vz + mu * (sz / m - vz);
+    }
+    if (APPLY)
+      v.vel[i] = make_float4(vx, vy, vz, 0.f);
+    else
+      v.delta[i] = make_float4(vx, vy, vz, m);
+  }
+}
+
+}  // namespace upbd

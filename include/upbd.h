@@ -366,6 +366,16 @@ int upbd_grid_build_noalloc(const void* pos4, const void* flags, int32_t n, int3
                             double cell_size, void* counts, void* offsets, void* entries,
                             void* stream);
 
+/* Neighbour-list statistics of the fluid gathers. The product build keeps
+ * each fluid particle's neighbour list across substeps and rebuilds the
+ * lists only when particles moved too far or the state changed from outside;
+ * the parity build walks the hash buckets every substep and reports zeros.
+ * rebuilds: substeps since creation whose density pass rebuilt every list;
+ * walkers: fluid particles whose density or xsph pass walked the buckets in
+ * the last substep stepped. Waits for the handle's stream. (No counterpart
+ * in the reference, which walks the buckets every substep.) */
+int upbd_list_stats(upbd_sim* sim, uint64_t* rebuilds, uint32_t* walkers);
+
 /* Kernels this handle has launched so far (each replay of a captured frame
  * counts its kernel nodes). Instrumentation for benchmarks. */
 uint64_t upbd_launch_count(upbd_sim* sim);
