@@ -35,7 +35,7 @@ constexpr int SCR_HEALTH = 6;      // UPBD_HEALTH_* bits
 constexpr int SCR_XMOVE = 7;       // largest movement the bounds pass recorded this substep (float bits)
 constexpr int SCR_REBUILD = 8;     // product build: this substep's density pass rebuilds every fluid list
 constexpr int SCR_DIRTY = 9;       // product build: the lists no longer describe the state (set by tools, culls)
-constexpr int SCR_WALKERS = 10;    // product build: particles that walked the buckets this substep
+constexpr int SCR_WALKERS = 10;    // product build: particles that walked for want of a usable list this substep
 constexpr int SCR_REBUILDS = 11;   // product build: substeps that rebuilt the lists (wraps at 2^32)
 constexpr int SCR_WORDS = 16;
 // mapped host words
@@ -262,8 +262,8 @@ constexpr uint32_t PF_DUP = 1u;    // two of the 27 buckets around the grid-time
 constexpr uint32_t PF_DUPF = 2u;   // the same for the cell at xsph time
 constexpr uint32_t PF_LOK = 4u;    // the list is complete (no lane overflowed, no coinciding buckets at the rebuild)
 constexpr uint32_t PF_LIST = 8u;   // this substep's density and displacement read the list
-// A rebuild follows a substep whose density and xsph passes walked for more
-// than F / VWALK_DIV particles.
+// A rebuild follows a substep whose density and xsph passes walked, for want
+// of a usable list, for more than F / VWALK_DIV particles.
 constexpr uint32_t VWALK_DIV = 512u;
 
 template <int G = GL>

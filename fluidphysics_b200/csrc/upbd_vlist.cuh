@@ -25,8 +25,10 @@
 // movement recorded in its 27 buckets does (every particle the reference
 // could count sits in one of them). Particles that fail walk the buckets
 // (without touching their lists). A rebuild follows a substep where more
-// than F / VWALK_DIV particles walked, and any change the lists cannot
-// follow (emit, drain, a state write, a cull: SCR_DIRTY).
+// than F / VWALK_DIV particles walked for want of a usable list (particles
+// whose 27 buckets coincide walk regardless and are not counted), and any
+// change the lists cannot follow (emit, drain, a state write, a cull:
+// SCR_DIRTY).
 #pragma once
 #include "upbd_device.cuh"
 
@@ -144,7 +146,9 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
   }
   rho = lane_sum<GLF>(rho);
   rhoNear = lane_sum<GLF>(rhoNear);
-  if (!rebuild) vl_count_walkers(v, walks, lane);
+  // a particle whose buckets coincide walks whatever the lists hold: it does
+  // not count towards a rebuild
+  if (!rebuild) vl_count_walkers(v, walks && !(pf & PF_DUP), lane);
   if (act && lane == 0) {
     const float2 d = make_float2(rho, rhoNear);
     v.density[i] = d;
@@ -374,7 +378,7 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
   sy = lane_sum<GLF>(sy);
   sz = lane_sum<GLF>(sz);
   m = lane_sum<GLF>(m);
-  vl_count_walkers(v, walks, lane);
+  vl_count_walkers(v, walks && !(pf & PF_DUPF), lane);
   if (act && lane == 0) {
     const float4 vi = v.vel[i];
     float vx = vi.x, vy = vi.y, vz = vi.z;

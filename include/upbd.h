@@ -372,7 +372,8 @@ int upbd_grid_build_noalloc(const void* pos4, const void* flags, int32_t n, int3
  * the parity build walks the hash buckets every substep and reports zeros.
  * rebuilds: substeps since creation whose density pass rebuilt every list;
  * walkers: fluid particles whose density or xsph pass walked the buckets in
- * the last substep stepped. Waits for the handle's stream. (No counterpart
+ * the last substep stepped for want of a usable list (those whose 27 buckets
+ * share a bucket always walk and are not counted). Waits for the handle's stream. (No counterpart
  * in the reference, which walks the buckets every substep.) */
 int upbd_list_stats(upbd_sim* sim, uint64_t* rebuilds, uint32_t* walkers);
 
