@@ -125,9 +125,9 @@ struct SimView {
   uint32_t* ccount;
   uint32_t* clist;
   // Product build: fluid neighbour lists kept across substeps (particle
-  // indices; lane l of fluid particle f = i - S keeps its entries at
-  // nbr[(l*NL + c) * F + f] and their number at ncount[l*F + f], reusing the
-  // parity build's per-substep list arrays), the position each list was
+  // indices; fluid particle f = i - S keeps its entries at nbr[c * F + f],
+  // c < NLT, and their number at ncount[f], reusing the parity build's
+  // per-substep list arrays), the position each list was
   // built at (xlist[f]), per-particle state bits (pfl, PF_* below) and a
   // particle-indexed copy of the velocities for xsph (ivel; w = 1 when the
   // particle changed cell after the grid build).
@@ -218,6 +218,7 @@ __device__ __forceinline__ bool buckets_coincide(const CellHash& ch, uint32_t ma
 constexpr int GL = 8;
 constexpr int GLF = 4;
 constexpr uint32_t NL = 32;  // density-pass neighbour-list entries kept per fluid lane (GLF * NL per particle)
+constexpr uint32_t NLT = NL * GLF;  // product build: entries of one fluid particle's list kept across substeps
 constexpr int DL = 2;        // threads per particle in the displacement pass
 // threads per grid slot of the displacement launch: the parity build's DL
 // threads over the density pass's per-substep lists, the product build's GLF
@@ -246,8 +247,9 @@ constexpr float XMOVE_REC = 0.25f;
 constexpr uint32_t NBR_IN = 0x80000000u;  // list entry flag: within H at density time (slots stay below 2^31)
 
 // Product build: neighbour lists kept across substeps (Verlet lists). At a
-// rebuild the density pass lists, per lane, every fluid candidate of its walk
-// within H * (1 + VSKIN) and records the particle's position. A later
+// rebuild the density pass lists every fluid particle within H * (1 + VSKIN)
+// (the 27 cells and the cells beyond them that the radius reaches) and
+// records the particle's position. A later
 // substep may read the list instead of walking the 27 buckets when the
 // particle's own movement since the rebuild plus the largest movement of any
 // particle that can be within H of it stays within VMOVE_FRAC of the skin
@@ -260,7 +262,7 @@ constexpr float VMOVE_REC = 0.25f;
 // pfl bits
 constexpr uint32_t PF_DUP = 1u;    // two of the 27 buckets around the grid-time cell coincide
 constexpr uint32_t PF_DUPF = 2u;   // the same for the cell at xsph time
-constexpr uint32_t PF_LOK = 4u;    // the list is complete (no lane overflowed, no coinciding buckets at the rebuild)
+constexpr uint32_t PF_LOK = 4u;    // the list is complete (it did not overflow at the rebuild)
 constexpr uint32_t PF_LIST = 8u;   // this substep's density and displacement read the list
 // A rebuild follows a substep whose density and xsph passes walked, for want
 // of a usable list, for more than F / VWALK_DIV particles.

@@ -16,9 +16,11 @@
 // holds whenever j is within H, and the others (ivel[j].w = 1) are checked
 // against the 27 buckets explicitly.
 //
-// When lists are complete. A rebuild (density pass, SCR_REBUILD) lists for
-// each lane every fluid candidate of its walk share within H * (1 + VSKIN)
-// and records the position. A list may be read when the particle's movement
+// When lists are complete. A rebuild (density pass, SCR_REBUILD) lists every
+// fluid particle within R = H * (1 + VSKIN): it walks the 27 cells and the
+// cells beyond them that R reaches (R is below two cell sizes), and takes a
+// candidate only at the visit of its own cell, so buckets met through two
+// cells list it once; it records the position. A list may be read when the particle's movement
 // since then, plus the largest movement of any particle that can be within H
 // of it, stays within the allowance VMOVE_FRAC * VSKIN * H: the scene-wide
 // largest recorded movement settles most particles; otherwise the largest
@@ -67,6 +69,18 @@ __device__ __forceinline__ void vl_count_walkers(const SimView& v, bool walks, i
   if (b != 0u && (threadIdx.x & 31) == 0) atomicAdd(&v.scratch[SCR_WALKERS], (uint32_t)__popc(b));
 }
 
+// Cell (cx, cy, cz) is the cell of p (Solver._hashPos's floor(p * (1/cs))).
+__device__ __forceinline__ bool vl_in_cell(const float4& p, double inv, double cx, double cy, double cz) {
+  return floor(__dmul_rn((double)p.x, inv)) == cx && floor(__dmul_rn((double)p.y, inv)) == cy &&
+         floor(__dmul_rn((double)p.z, inv)) == cz;
+}
+
+// Hash component (Solver._hash) of cell coordinate c + o, o in -2..2, from
+// the five precomputed ones.
+__device__ __forceinline__ int32_t vl_sel(int o, int32_t m2, int32_t m1, int32_t z0, int32_t p1, int32_t p2) {
+  return (o == -2) ? m2 : ((o == -1) ? m1 : ((o == 0) ? z0 : ((o == 1) ? p1 : p2)));
+}
+
 // fluidDensity (src/gpu/wgsl.js:254-279); at a rebuild also writes the lists.
 __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const unsigned FULL = 0xffffffffu;
@@ -74,6 +88,7 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
   if (rebuild && vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GLF - 1);
+  const int g = (int)threadIdx.x / GLF;
   uint32_t myslot, i;
   bool act;
   slot_group(v, t, myslot, i, act);
@@ -97,12 +112,103 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
   }
   const bool walks = act && !listed;
   float rho = 0.f, rhoNear = 0.f;
-  uint32_t over = 0u;
-  if (__any_sync(FULL, walks)) {
-    const float HS = H * (1.0f + VSKIN), HS2 = HS * HS;
-    uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
-    const float4* __restrict__ spos = v.spos;
-    uint32_t cnt = 0;
+  const float4* __restrict__ spos = v.spos;
+  uint32_t lcount = 0;  // list length (rebuild)
+  if (rebuild) {
+    // The reference's density over the 27 cells (every bucket visit counted,
+    // coinciding buckets included) and, for the list, every fluid candidate
+    // within R met at the visit of its own cell (so a bucket met through two
+    // cells lists it once); then the cells past the 27 that R reaches. The
+    // group's lanes step together and place their entries by a ballot, so the
+    // list holds the candidates in walk order (deterministic sums).
+    const double inv = P->inv_cell;
+    const double cx = floor(__dmul_rn((double)pi.x, inv)), cy = floor(__dmul_rn((double)pi.y, inv)),
+                 cz = floor(__dmul_rn((double)pi.z, inv));
+    const float R = H * (1.0f + VSKIN), R2 = R * R;
+    uint32_t* __restrict__ lst = v.nbr + f;
+    const unsigned gmask = 0xFu << ((threadIdx.x & 31) & ~(unsigned)(GLF - 1));
+    const unsigned lt = gmask & ((1u << (threadIdx.x & 31)) - 1u);  // group lanes below this one
+    auto place = [&](bool kp, uint32_t e) {
+      const unsigned bal = __ballot_sync(gmask, kp);
+      if (kp) {
+        const uint32_t c = lcount + (uint32_t)__popc(bal & lt);
+        if (c < NLT) lst[(size_t)c * FS] = __ldg(&v.entries[e]);
+      }
+      lcount += (uint32_t)__popc(bal);
+    };
+    const uint32_t run = walk_tables<0, GLF>(v, ch, lane, act, g);
+    uint32_t k = 0, next = s_walk_off[g][1], base = s_walk_base[g][0];
+    for (uint32_t c0 = 0; c0 < run; c0 += GLF) {  // the same trip count for the group's lanes
+      const uint32_t c = c0 + (uint32_t)lane;
+      bool kp = false;
+      uint32_t e = 0;
+      if (c < run) {
+        while (c >= next) {
+          k++;
+          next = s_walk_off[g][k + 1];
+          base = s_walk_base[g][k];
+        }
+        e = base + c;
+        const float4 pj = spos[e];
+        const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+        const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+        const bool in = (e != myslot) && (d2 < H2);
+        const float q = 1.0f - approx_sqrt(d2) * invH;
+        const float qq = in ? q * q : 0.0f;
+        rho = rho + qq;
+        rhoNear = rhoNear + qq * q;
+        if (e != myslot && d2 < R2) {
+          const int a = (int)k / 9 - 1, b = ((int)k / 3) % 3 - 1, cc = (int)k % 3 - 1;
+          kp = vl_in_cell(pj, inv, cx + a, cy + b, cz + cc);
+        }
+      }
+      place(kp, e);
+    }
+    __syncwarp();  // the tables are rewritten by the next walk
+    if (act) {
+      // reach of R past the 27 cells, in cells (R is below two cells)
+      const double ext = (double)R * inv - 1.0 + 1e-3, rc2 = ((double)R * inv) * ((double)R * inv) * 1.0001;
+      const double fx = __dmul_rn((double)pi.x, inv) - cx, fy = __dmul_rn((double)pi.y, inv) - cy,
+                   fz = __dmul_rn((double)pi.z, inv) - cz;
+      const int lox = (fx < ext) ? -2 : -1, hix = (1.0 - fx < ext) ? 2 : 1;
+      const int loy = (fy < ext) ? -2 : -1, hiy = (1.0 - fy < ext) ? 2 : 1;
+      const int loz = (fz < ext) ? -2 : -1, hiz = (1.0 - fz < ext) ? 2 : 1;
+      if (lox < -1 || hix > 1 || loy < -1 || hiy > 1 || loz < -1 || hiz > 1) {
+        const int32_t xm2 = js_toint32(__dmul_rn(__dadd_rn(cx, -2.0), 92837111.0));
+        const int32_t xp2 = js_toint32(__dmul_rn(__dadd_rn(cx, 2.0), 92837111.0));
+        const int32_t ym2 = js_toint32(__dmul_rn(__dadd_rn(cy, -2.0), 689287499.0));
+        const int32_t yp2 = js_toint32(__dmul_rn(__dadd_rn(cy, 2.0), 689287499.0));
+        const int32_t zm2 = js_toint32(__dmul_rn(__dadd_rn(cz, -2.0), 283923481.0));
+        const int32_t zp2 = js_toint32(__dmul_rn(__dadd_rn(cz, 2.0), 283923481.0));
+        const uint32_t mask = (uint32_t)v.T - 1u;
+        for (int a = lox; a <= hix; a++)
+          for (int b = loy; b <= hiy; b++)
+            for (int c = loz; c <= hiz; c++) {
+              if (a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1) continue;  // one of the 27
+              // distance (in cells) from the particle to the cell's box
+              const double gx = (a < 0) ? fx + (double)(-a - 1) : ((a > 0) ? (1.0 - fx) + (double)(a - 1) : 0.0);
+              const double gy = (b < 0) ? fy + (double)(-b - 1) : ((b > 0) ? (1.0 - fy) + (double)(b - 1) : 0.0);
+              const double gz = (c < 0) ? fz + (double)(-c - 1) : ((c > 0) ? (1.0 - fz) + (double)(c - 1) : 0.0);
+              if (gx * gx + gy * gy + gz * gz > rc2) continue;
+              const uint32_t h = (uint32_t)(vl_sel(a, xm2, ch.hx[0], ch.hx[1], ch.hx[2], xp2) ^
+                                            vl_sel(b, ym2, ch.hy[0], ch.hy[1], ch.hy[2], yp2) ^
+                                            vl_sel(c, zm2, ch.hz[0], ch.hz[1], ch.hz[2], zp2)) & mask;
+              const uint32_t s0 = __ldg(&v.start[h]), s1 = __ldg(&v.fend[h]);
+              for (uint32_t e0 = s0; e0 < s1; e0 += GLF) {  // the same trip count for the group's lanes
+                const uint32_t e = e0 + (uint32_t)lane;
+                bool kp = false;
+                if (e < s1) {
+                  const float4 pj = spos[e];
+                  const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+                  kp = dot3(ex, ey, ez, ex, ey, ez) < R2 &&
+                       vl_in_cell(pj, inv, cx + (double)a, cy + (double)b, cz + (double)c);
+                }
+                place(kp, e);
+              }
+            }
+      }
+    }
+  } else if (__any_sync(FULL, walks)) {
     lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
       const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
       const float d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -111,24 +217,15 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
       const float qq = in ? q * q : 0.0f;
       rho = rho + qq;
       rhoNear = rhoNear + qq * q;
-      if (rebuild) {
-        const bool keep = (e != myslot) && (d2 < HS2);
-        if (keep && cnt < NL) lst[cnt * FS] = __ldg(&v.entries[e]);
-        cnt += keep ? 1u : 0u;
-      }
     });
-    if (rebuild && walks) v.ncount[lane * FS + f] = cnt;
-    over = (cnt > NL) ? 1u : 0u;
-#pragma unroll
-    for (int d = 1; d < GLF; d <<= 1) over |= __shfl_xor_sync(FULL, over, d);
   }
-  if (listed) {
-    const uint32_t n = v.ncount[lane * FS + f];
-    const uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
+  if (listed) {  // lane l reads entries l, l + GLF, ...
+    const uint32_t n = v.ncount[f];
+    const uint32_t* __restrict__ lst = v.nbr + f;
     const float4* __restrict__ pos = v.pos;
-    for (uint32_t c = 0; c < n; c += 2) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[c * FS]);
-      const uint32_t j1 = (c + 1 < n) ? __ldg(&lst[(c + 1) * FS]) : j0;
+    for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
+      const uint32_t j0 = __ldg(&lst[(size_t)c * FS]);
+      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * FS]) : j0;
       const float4 p0 = pos[j0], p1 = pos[j1];
       float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
       float d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -139,7 +236,7 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
       ex = p1.x - pi.x; ey = p1.y - pi.y; ez = p1.z - pi.z;
       d2 = dot3(ex, ey, ez, ex, ey, ez);
       q = 1.0f - approx_sqrt(d2) * invH;
-      qq = (d2 < H2 && c + 1 < n) ? q * q : 0.0f;
+      qq = (d2 < H2 && c + GLF < n) ? q * q : 0.0f;
       rho = rho + qq;
       rhoNear = rhoNear + qq * q;
     }
@@ -155,8 +252,10 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
     v.sdens[myslot] = d;
     uint32_t npf = pf;
     if (rebuild) {
+      const uint32_t cnt = lcount;
+      v.ncount[f] = cnt;
       v.xlist[f] = pi;
-      npf = (over || (pf & PF_DUP)) ? (npf & ~PF_LOK) : (npf | PF_LOK);
+      npf = (cnt > NLT) ? (npf & ~PF_LOK) : (npf | PF_LOK);
     }
     npf = listed ? (npf | PF_LIST) : (npf & ~PF_LIST);
     v.pfl[i] = npf;
@@ -213,20 +312,20 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
                            if (e != myslot) pair(c.p, c.d);
                          });
   }
-  if (listed) {
+  if (listed) {  // lane l reads entries l, l + GLF, ...
     const uint32_t FS = (uint32_t)v.F;
     const uint32_t f = i - (uint32_t)v.S;
-    const uint32_t n = v.ncount[lane * FS + f];
-    const uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
+    const uint32_t n = v.ncount[f];
+    const uint32_t* __restrict__ lst = v.nbr + f;
     const float4* __restrict__ pos = v.pos;
     const float2* __restrict__ dens = v.density;
-    for (uint32_t c = 0; c < n; c += 2) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[c * FS]);
-      const uint32_t j1 = (c + 1 < n) ? __ldg(&lst[(c + 1) * FS]) : j0;
+    for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
+      const uint32_t j0 = __ldg(&lst[(size_t)c * FS]);
+      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * FS]) : j0;
       const float4 p0 = pos[j0], p1 = pos[j1];
       const float2 d0 = dens[j0], d1 = dens[j1];
       pair(p0, d0);
-      if (c + 1 < n) pair(p1, d1);
+      if (c + GLF < n) pair(p1, d1);
     }
   }
 #pragma unroll
@@ -350,16 +449,16 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
                            sz = sz + (in ? c.v.z : 0.f); m = m + (in ? 1.0f : 0.f);
                          });
   }
-  if (listed) {
+  if (listed) {  // lane l reads entries l, l + GLF, ...
     const uint32_t FS = (uint32_t)v.F;
     const uint32_t f = i - (uint32_t)v.S;
-    const uint32_t n = v.ncount[lane * FS + f];
-    const uint32_t* __restrict__ lst = v.nbr + (size_t)lane * NL * FS + f;
+    const uint32_t n = v.ncount[f];
+    const uint32_t* __restrict__ lst = v.nbr + f;
     const float4* __restrict__ pos = v.pos;
     const float4* __restrict__ ivel = v.ivel;
-    for (uint32_t c = 0; c < n; c += 2) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[c * FS]);
-      const uint32_t j1 = (c + 1 < n) ? __ldg(&lst[(c + 1) * FS]) : j0;
+    for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
+      const uint32_t j0 = __ldg(&lst[(size_t)c * FS]);
+      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * FS]) : j0;
       const float4 p0 = pos[j0], p1 = pos[j1];
       const float4 u0 = ivel[j0], u1 = ivel[j1];
       float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
@@ -368,7 +467,7 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
       sx = sx + (in ? u0.x : 0.f); sy = sy + (in ? u0.y : 0.f); sz = sz + (in ? u0.z : 0.f);
       m = m + (in ? 1.0f : 0.f);
       ex = p1.x - pi.x; ey = p1.y - pi.y; ez = p1.z - pi.z;
-      in = (c + 1 < n) && dot3(ex, ey, ez, ex, ey, ez) < H2;
+      in = (c + GLF < n) && dot3(ex, ey, ez, ex, ey, ez) < H2;
       if (in && u1.w != 0.f) in = vl_member(v, P, pi, j1);
       sx = sx + (in ? u1.x : 0.f); sy = sy + (in ? u1.y : 0.f); sz = sz + (in ? u1.z : 0.f);
       m = m + (in ? 1.0f : 0.f);
