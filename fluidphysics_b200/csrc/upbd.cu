@@ -1240,18 +1240,28 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
   return UPBD_OK;
 }
 
-int upbd_list_stats(upbd_sim* s, uint64_t* rebuilds, uint32_t* walkers) {
-  if (!s || !rebuilds || !walkers) return UPBD_ERR_INVALID;
+int upbd_list_stats(upbd_sim* s, upbd_list_info* out) {
+  if (!s || !out) return UPBD_ERR_INVALID;
   cudaSetDevice(s->device);
+  std::memset(out, 0, sizeof(*out));
+#ifndef UPBD_PARITY_BUILD
+  UPBD_CK(s, cudaMemsetAsync(s->v.scratch + SCR_CENSUS, 0, 4 * sizeof(uint32_t), s->stream));
+  if (s->v.F > 0) {
+    k_list_census<<<blocks_for(s->v.F), 256, 0, s->stream>>>(s->v);
+    UPBD_KCK(s);
+  }
   uint32_t w[SCR_WORDS];
   UPBD_CK(s, cudaMemcpyAsync(w, s->v.scratch, sizeof(w), cudaMemcpyDeviceToHost, s->stream));
   UPBD_CK(s, cudaStreamSynchronize(s->stream));
-#ifdef UPBD_PARITY_BUILD
-  *rebuilds = 0;
-  *walkers = 0;
-#else
-  *rebuilds = w[SCR_REBUILDS];
-  *walkers = w[SCR_WALKERS];
+  uint32_t act = 0;
+  int rc = upbd_active_count(s, &act);
+  if (rc) return rc;
+  out->rebuilds = w[SCR_REBUILDS];
+  out->walkers = w[SCR_WALKERS];
+  out->listed = w[SCR_CENSUS];
+  out->complete = w[SCR_CENSUS + 1];
+  out->max_len = w[SCR_CENSUS + 2];
+  out->mean_len = act ? (double)w[SCR_CENSUS + 3] / act : 0.0;
 #endif
   return UPBD_OK;
 }

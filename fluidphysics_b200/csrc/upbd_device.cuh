@@ -37,6 +37,7 @@ constexpr int SCR_REBUILD = 8;     // product build: this substep's density pass
 constexpr int SCR_DIRTY = 9;       // product build: the lists no longer describe the state (set by tools, culls)
 constexpr int SCR_WALKERS = 10;    // product build: particles that walked for want of a usable list this substep
 constexpr int SCR_REBUILDS = 11;   // product build: substeps that rebuilt the lists (wraps at 2^32)
+constexpr int SCR_CENSUS = 12;     // product build: list census (listed, complete, longest, total length)
 constexpr int SCR_WORDS = 16;
 // mapped host words
 constexpr int HM_ACTIVE = 0;

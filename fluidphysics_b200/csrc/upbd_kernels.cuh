@@ -287,6 +287,31 @@ __global__ void k_grab_release(SimView v) {
   if (i < v.S) v.flags[i] &= ~F_GRABBED;
 }
 
+// Census of the product build's fluid lists into scratch[SCR_CENSUS..+3]
+// (cleared by the caller): particles that read their list in the last
+// density pass, particles holding a complete list, the longest list, the
+// total length.
+__global__ void k_list_census(SimView v) {
+  const int i = v.S + (int)UPBD_TID;
+  uint32_t listed = 0, complete = 0, len = 0;
+  if (i < v.N && (v.flags[i] & F_ACTIVE) && v.pfl) {
+    const uint32_t pf = v.pfl[i];
+    listed = (pf & PF_LIST) ? 1u : 0u;
+    complete = (pf & PF_LOK) ? 1u : 0u;
+    len = v.ncount[i - v.S];
+  }
+  listed = __reduce_add_sync(0xffffffffu, listed);
+  complete = __reduce_add_sync(0xffffffffu, complete);
+  const uint32_t mx = __reduce_max_sync(0xffffffffu, len);
+  len = __reduce_add_sync(0xffffffffu, len);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&v.scratch[SCR_CENSUS], listed);
+    atomicAdd(&v.scratch[SCR_CENSUS + 1], complete);
+    atomicMax(&v.scratch[SCR_CENSUS + 2], mx);
+    atomicAdd(&v.scratch[SCR_CENSUS + 3], len);
+  }
+}
+
 // GpuSim.clearFluid, src/gpu/sim.js:294-297
 __global__ void k_drain(SimView v) {
   const int i = v.S + (int)UPBD_TID;
