@@ -251,13 +251,17 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
     v.density[i] = d;
     v.sdens[myslot] = d;
     uint32_t npf = pf;
+    bool use = listed;
     if (rebuild) {
       const uint32_t cnt = lcount;
       v.ncount[f] = cnt;
       v.xlist[f] = pi;
       npf = (cnt > NLT) ? (npf & ~PF_LOK) : (npf | PF_LOK);
+      // the fresh list holds exactly this substep's pairs when complete and
+      // no two of the 27 buckets coincide: the displacement pass reads it
+      use = cnt <= NLT && !(pf & PF_DUP);
     }
-    npf = listed ? (npf | PF_LIST) : (npf & ~PF_LIST);
+    npf = use ? (npf | PF_LIST) : (npf & ~PF_LIST);
     v.pfl[i] = npf;
   }
 }
