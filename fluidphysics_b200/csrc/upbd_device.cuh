@@ -32,7 +32,8 @@ constexpr int SCR_CUT = 3;         // constraints cut by the last wedge
 constexpr int SCR_ACTIVE = 4;      // active-fluid partial sums
 constexpr int SCR_DONE = 5;        // blocks finished (last-block pattern)
 constexpr int SCR_HEALTH = 6;      // UPBD_HEALTH_* bits
-constexpr int SCR_XMOVE = 7;       // largest movement the bounds pass recorded this substep (float bits)
+constexpr int SCR_XMOVE = 7;       // largest movement the bounds pass recorded this substep (float bits;
+                                   // product build: of the particles below VFAST)
 constexpr int SCR_REBUILD = 8;     // product build: this substep's density pass rebuilds every fluid list
 constexpr int SCR_DIRTY = 9;       // product build: the lists no longer describe the state (set by tools, culls)
 constexpr int SCR_WALKERS = 10;    // product build: particles that walked for want of a usable list this substep
@@ -125,16 +126,27 @@ struct SimView {
   float4* sfp;
   uint32_t* ccount;
   uint32_t* clist;
-  // Product build: fluid neighbour lists kept across substeps (particle
-  // indices; fluid particle f = i - S keeps its entries at nbr[c * F + f],
-  // c < NLT, and their number at ncount[f], reusing the parity build's
-  // per-substep list arrays), the position each list was
-  // built at (xlist[f]), per-particle state bits (pfl, PF_* below) and a
-  // particle-indexed copy of the velocities for xsph (ivel; w = 1 when the
-  // particle changed cell after the grid build).
+  // Product build: fluid neighbour lists kept across substeps. They live in
+  // the "rank" order of the last rebuild (the grid's slot order at that
+  // substep, so neighbours sit close together): ep[r] is the particle of
+  // rank r (NO_RANK past the active ones), erank[i] the rank of particle i.
+  // The list of rank r holds ranks, nbr[c * N + r] for c < ncount[r] <= NLT
+  // (reusing the parity build's per-substep list arrays), and xlist[r] is the
+  // position it was built at. The gathers read their neighbours from
+  // rank-ordered copies: epos (grid-time positions, then from the bounds
+  // pass on the final ones), edens (density) and evel (velocity after the
+  // velocity pass; w = 1 when the particle changed cell after the grid
+  // build). pfl holds per-particle state bits (PF_* below); bfast marks the
+  // buckets around particles that moved far since the rebuild (cleared by
+  // the scan every substep).
+  uint32_t* ep;
+  uint32_t* erank;
   float4* xlist;
+  float4* epos;
+  float2* edens;
+  float4* evel;
   uint32_t* pfl;
-  float4* ivel;
+  uint32_t* bfast;
   uint32_t* scratch;
   uint32_t* host_mapped;
   int S, N1, dim1, dim2, F, N, C, NT, T, num_tiles;
@@ -260,11 +272,18 @@ constexpr uint32_t NBR_IN = 0x80000000u;  // list entry flag: within H at densit
 constexpr float VSKIN = 0.25f;
 constexpr float VMOVE_FRAC = 0.9f;
 constexpr float VMOVE_REC = 0.25f;
+// A particle that moved more than VFAST * the allowance since the rebuild
+// marks the 27 buckets around its cell (bfast) instead of raising the
+// scene-wide bound SCR_XMOVE, so a few fast particles send only their
+// neighbours to the per-bucket test.
+constexpr float VFAST = 0.5f;
+constexpr uint32_t NO_RANK = 0xffffffffu;
 // pfl bits
 constexpr uint32_t PF_DUP = 1u;    // two of the 27 buckets around the grid-time cell coincide
 constexpr uint32_t PF_DUPF = 2u;   // the same for the cell at xsph time
 constexpr uint32_t PF_LOK = 4u;    // the list is complete (it did not overflow at the rebuild)
 constexpr uint32_t PF_LIST = 8u;   // this substep's density and displacement read the list
+constexpr uint32_t PF_MOVED = 16u; // the particle changed cell after this substep's grid build
 // A rebuild follows a substep whose density and xsph passes walked, for want
 // of a usable list, for more than F / VWALK_DIV particles.
 constexpr uint32_t VWALK_DIV = 512u;

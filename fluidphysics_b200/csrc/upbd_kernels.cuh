@@ -296,9 +296,10 @@ __global__ void k_list_census(SimView v) {
   uint32_t listed = 0, complete = 0, len = 0;
   if (i < v.N && (v.flags[i] & F_ACTIVE) && v.pfl) {
     const uint32_t pf = v.pfl[i];
+    const uint32_t r = v.erank[i];
     listed = (pf & PF_LIST) ? 1u : 0u;
     complete = (pf & PF_LOK) ? 1u : 0u;
-    len = v.ncount[i - v.S];
+    len = (r < (uint32_t)v.N) ? v.ncount[r] : 0u;
   }
   listed = __reduce_add_sync(0xffffffffu, listed);
   complete = __reduce_add_sync(0xffffffffu, complete);

@@ -178,6 +178,12 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
       *reinterpret_cast<uint4*>(v.bmove + t0) = z;
       *reinterpret_cast<uint4*>(v.bmove + t0 + 4) = z;
     }
+#ifndef UPBD_PARITY_BUILD
+    if (v.bfast) {
+      *reinterpret_cast<uint4*>(v.bfast + t0) = z;
+      *reinterpret_cast<uint4*>(v.bfast + t0 + 4) = z;
+    }
+#endif
   } else {
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -187,6 +193,9 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
         if (v.fend) v.fend[idx] = r[k];
         v.counts[idx] = 0u;
         if (v.bmove) v.bmove[idx] = 0u;
+#ifndef UPBD_PARITY_BUILD
+        if (v.bfast) v.bfast[idx] = 0u;
+#endif
       }
     }
   }
@@ -1010,7 +1019,8 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   if (!iSolid) record_move(v, P, i, sl, o, p);
   const float moved = 0.f;
 #else
-  const float moved = (!iSolid && vl_record(v, P, i, sl, o, p)) ? 1.f : 0.f;
+  const uint32_t erk = (!iSolid && P->use_lists) ? v.erank[i] : NO_RANK;
+  const float moved = (erk != NO_RANK && vl_record(v, P, i, erk, o, p)) ? 1.f : 0.f;
   if (culled) atomicOr(&v.scratch[SCR_DIRTY], 1u);  // the next substep rebuilds the lists
 #endif
   v.spos[sl] = p;
@@ -1021,7 +1031,7 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
     const float4 vv = v.vel[i];
     v.svel[sl] = vv;
 #ifndef UPBD_PARITY_BUILD
-    v.ivel[i] = make_float4(vv.x, vv.y, vv.z, moved);
+    if (!iSolid && erk != NO_RANK) v.evel[erk] = make_float4(vv.x, vv.y, vv.z, moved);
 #endif
     return;
   }
@@ -1043,7 +1053,8 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   v.vel[i] = nv;
   v.svel[sl] = nv;
 #ifndef UPBD_PARITY_BUILD
-  v.ivel[i] = make_float4(vx, vy, vz, moved);  // w: changed cell after the grid build (xsph's list rule)
+  // w: changed cell after the grid build (xsph's list rule)
+  if (!iSolid && erk != NO_RANK) v.evel[erk] = make_float4(vx, vy, vz, moved);
 #else
   (void)moved;
 #endif

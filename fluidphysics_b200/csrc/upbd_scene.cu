@@ -194,9 +194,14 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.sfp = cv.take<float4>(v.N);
   L.smove = cv.take<float>(v.N);
   L.bmove = cv.take<uint32_t>(v.T);
-  L.xlist = cv.take<float4>(std::max(v.F, 1));
+  L.ep = cv.take<uint32_t>(v.N);
+  L.erank = cv.take<uint32_t>(v.N);
+  L.xlist = cv.take<float4>(v.N);
+  L.epos = cv.take<float4>(v.N);
+  L.edens = cv.take<float2>(v.N);
+  L.evel = cv.take<float4>(v.N);
   L.pfl = cv.take<uint32_t>(v.N);
-  L.ivel = cv.take<float4>(v.N);
+  L.bfast = cv.take<uint32_t>(v.T);
   L.scr = cv.take<uint32_t>(SCR_WORDS);
   L.par = cv.take<DevParams>(1);
   L.bytes = cv.off;
@@ -238,9 +243,14 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.sfp = (float4*)(base + L.sfp);
   v.smove = (float*)(base + L.smove);
   v.bmove = (uint32_t*)(base + L.bmove);
+  v.ep = (uint32_t*)(base + L.ep);
+  v.erank = (uint32_t*)(base + L.erank);
   v.xlist = (float4*)(base + L.xlist);
+  v.epos = (float4*)(base + L.epos);
+  v.edens = (float2*)(base + L.edens);
+  v.evel = (float4*)(base + L.evel);
   v.pfl = (uint32_t*)(base + L.pfl);
-  v.ivel = (float4*)(base + L.ivel);
+  v.bfast = (uint32_t*)(base + L.bfast);
   v.scratch = (uint32_t*)(base + L.scr);
   if (params) *params = (DevParams*)(base + L.par);
 }

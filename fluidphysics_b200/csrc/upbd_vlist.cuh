@@ -13,24 +13,31 @@
 // fluid j within H, once. xsph runs after the fluid moved but on the grid
 // built before: j counts when its grid-time bucket is among the 27 buckets
 // of i's current cell; for a j that kept its cell since the grid build that
-// holds whenever j is within H, and the others (ivel[j].w = 1) are checked
+// holds whenever j is within H, and the others (evel[.].w = 1) are checked
 // against the 27 buckets explicitly.
 //
 // When lists are complete. A rebuild (density pass, SCR_REBUILD) lists every
 // fluid particle within R = H * (1 + VSKIN): it walks the 27 cells and the
 // cells beyond them that R reaches (R is below two cell sizes), and takes a
 // candidate only at the visit of its own cell, so buckets met through two
-// cells list it once; it records the position. A list may be read when the particle's movement
-// since then, plus the largest movement of any particle that can be within H
-// of it, stays within the allowance VMOVE_FRAC * VSKIN * H: the scene-wide
-// largest recorded movement settles most particles; otherwise the largest
-// movement recorded in its 27 buckets does (every particle the reference
-// could count sits in one of them). Particles that fail walk the buckets
-// (without touching their lists). A rebuild follows a substep where more
-// than F / VWALK_DIV particles walked for want of a usable list (particles
-// whose 27 buckets coincide walk regardless and are not counted), and any
-// change the lists cannot follow (emit, drain, a state write, a cull:
-// SCR_DIRTY).
+// cells list it once; it records the position. A list may be read when the
+// particle's movement since then, plus the largest movement of any particle
+// that can be within H of it, stays within the allowance VMOVE_FRAC * VSKIN
+// * H. The scene-wide largest movement of the particles below VFAST * the
+// allowance (SCR_XMOVE) settles most particles; the faster ones mark the 27
+// buckets around them (bfast), and a particle in a marked bucket, or one
+// that the scene-wide bound does not settle, takes the largest movement
+// recorded in its 27 buckets (every particle the reference could count sits
+// in one of them). Particles that fail walk the buckets (without touching
+// their lists). A rebuild follows a substep where more than F / VWALK_DIV
+// particles walked for want of a usable list (particles whose 27 buckets
+// coincide walk regardless and are not counted), and any change the lists
+// cannot follow (emit, drain, a state write, a cull: SCR_DIRTY).
+//
+// Order. The gathers run their groups in the rank order of the last rebuild
+// (the grid's slot order then: group r takes particle ep[r]) and read their
+// own and their neighbours' data from rank-ordered copies, so list entries
+// and neighbour loads stay close together in memory between rebuilds.
 #pragma once
 #include "upbd_device.cuh"
 
@@ -69,6 +76,76 @@ __device__ __forceinline__ void vl_count_walkers(const SimView& v, bool walks, i
   if (b != 0u && (threadIdx.x & 31) == 0) atomicAdd(&v.scratch[SCR_WALKERS], (uint32_t)__popc(b));
 }
 
+// Records movement m of a fluid particle whose cell is that of p and grid
+// bucket h: above VMOVE_REC * the allowance into bmove[h]; above VFAST * the
+// allowance it marks the 27 buckets around p's cell, else it raises the
+// scene-wide SCR_XMOVE (one atomic per warp). am: the lanes that call it.
+__device__ __forceinline__ void vl_note_move(const SimView& v, const DevParams* __restrict__ P, unsigned am, float m,
+                                             uint32_t h, const float4& p) {
+  const float allow = vl_allowance(P);
+  const bool rec = m > VMOVE_REC * allow;
+  const bool fast = m > VFAST * allow;
+  if (rec) atomicMax(&v.bmove[h], __float_as_uint(m));
+  if (fast) {
+    CellHash ch;
+    ch.init(p.x, p.y, p.z, P->inv_cell);
+    const uint32_t mask = (uint32_t)v.T - 1u;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) v.bfast[ch.bucket(a, b, c, mask)] = 1u;
+  }
+  const uint32_t wm = __reduce_max_sync(am, (rec && !fast) ? __float_as_uint(m) : 0u);
+  if (wm != 0u && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&v.scratch[SCR_XMOVE], wm);
+}
+
+// Grid-time record by the rank fix-up (not at a rebuild, when the density
+// pass itself rewrites the rank copies): the position copy for the density
+// and displacement passes, and the movement since the list build.
+__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h) {
+  const unsigned am = __activemask();  // the lanes that reach the warp reduction below
+  const uint32_t r = v.erank[i];
+  float m = 0.f;
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (r != NO_RANK) {
+    p = v.pos[i];
+    v.epos[r] = p;
+    m = vl_dist(p, v.xlist[r]);
+  }
+  vl_note_move(v, P, am, m, h, p);
+}
+
+// Final-time record by the bounds pass for fluid particle i of rank r: its
+// final position copy, how far it moved since its list was built (smove[r]
+// and the bucket / scene records), and whether its final cell differs from
+// its grid-time cell o (returned, and PF_MOVED; then PF_DUPF is tested for
+// the new cell).
+__device__ __forceinline__ bool vl_record(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t r,
+                                          const float4& o, const float4& p) {
+  const unsigned am = __activemask();  // the lanes that reach the warp reduction below
+  v.epos[r] = p;
+  const float m = vl_dist(p, v.xlist[r]);
+  v.smove[r] = m;
+  vl_note_move(v, P, am, m, v.cell[i], p);
+  const double inv = P->inv_cell;
+  const bool same = floor(__dmul_rn((double)o.x, inv)) == floor(__dmul_rn((double)p.x, inv)) &&
+                    floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
+                    floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
+  const uint32_t pf = v.pfl[i];
+  bool dupf = (pf & PF_DUP) != 0u;
+  if (!same) {
+    CellHash ch;
+    ch.init(p.x, p.y, p.z, inv);
+    dupf = buckets_coincide(ch, (uint32_t)v.T - 1u);
+  }
+  uint32_t npf = dupf ? (pf | PF_DUPF) : (pf & ~PF_DUPF);
+  npf = same ? (npf & ~PF_MOVED) : (npf | PF_MOVED);
+  v.pfl[i] = npf;
+  return !same;
+}
+
 // Cell (cx, cy, cz) is the cell of p (Solver._hashPos's floor(p * (1/cs))).
 __device__ __forceinline__ bool vl_in_cell(const float4& p, double inv, double cx, double cy, double cz) {
   return floor(__dmul_rn((double)p.x, inv)) == cx && floor(__dmul_rn((double)p.y, inv)) == cy &&
@@ -81,27 +158,48 @@ __device__ __forceinline__ int32_t vl_sel(int o, int32_t m2, int32_t m1, int32_t
   return (o == -2) ? m2 : ((o == -1) ? m1 : ((o == 0) ? z0 : ((o == 1) ? p1 : p2)));
 }
 
-// fluidDensity (src/gpu/wgsl.js:254-279); at a rebuild also writes the lists.
+// The particle of group r (rank r of the last rebuild, or slot r of this
+// substep's grid when `slots`), its slot, and whether it is active fluid.
+__device__ __forceinline__ void vl_group(const SimView& v, uint32_t r, bool slots, uint32_t& i, uint32_t& slot,
+                                         bool& fluid) {
+  const uint32_t nact = __ldg(&v.start[v.T]);
+  if (slots) {
+    i = (r < nact) ? v.entries[r] : NO_RANK;
+    slot = r;
+  } else {
+    i = (r < (uint32_t)v.N) ? v.ep[r] : NO_RANK;
+    slot = (i != NO_RANK) ? v.slot[i] : 0u;
+  }
+  fluid = i != NO_RANK && i >= (uint32_t)v.S;
+}
+
+// fluidDensity (src/gpu/wgsl.js:254-279); a rebuild also sets the rank
+// order to this substep's grid order and writes the lists.
 __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const unsigned FULL = 0xffffffffu;
   const bool rebuild = v.scratch[SCR_REBUILD] != 0u;  // one value for the whole scene
   if (rebuild && vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GLF - 1);
-  const int g = (int)threadIdx.x / GLF;
-  uint32_t myslot, i;
+  const uint32_t r = t / GLF;  // this group's rank
+  const bool slots = rebuild || !P->use_lists;
+  uint32_t i, myslot;
   bool act;
-  slot_group(v, t, myslot, i, act);
+  vl_group(v, r, slots, i, myslot, act);
+  if (rebuild && lane == 0 && r < (uint32_t)v.N) {  // the new rank order
+    v.ep[r] = i;
+    if (i != NO_RANK) v.erank[i] = r;
+  }
   if (!__any_sync(FULL, act)) return;
-  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const uint32_t FS = (uint32_t)v.F;
-  const uint32_t f = act ? i - (uint32_t)v.S : 0u;
+  const float4 pi = act ? (slots ? v.spos[myslot] : v.epos[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t NS = (uint32_t)v.N;
   const uint32_t pf = act ? v.pfl[i] : 0u;
   const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
   const float allow = vl_allowance(P), rec = VMOVE_REC * allow;
-  const bool cand = act && !rebuild && P->use_lists && (pf & (PF_LOK | PF_DUP)) == PF_LOK;
-  const float mv = cand ? vl_dist(pi, v.xlist[f]) : 0.f;
-  const bool quick = cand && mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
+  const bool cand = act && !slots && (pf & (PF_LOK | PF_DUP)) == PF_LOK;
+  const float mv = cand ? vl_dist(pi, v.xlist[r]) : 0.f;
+  const bool quick = cand && mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow &&
+                     v.bfast[v.cell[i]] == 0u;
   const bool need = cand && !quick && mv + rec <= allow;
   bool listed = quick;
   CellHash ch;
@@ -120,22 +218,24 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
     // within R met at the visit of its own cell (so a bucket met through two
     // cells lists it once); then the cells past the 27 that R reaches. The
     // group's lanes step together and place their entries by a ballot, so the
-    // list holds the candidates in walk order (deterministic sums).
+    // list holds the candidates in walk order (deterministic sums). At a
+    // rebuild a candidate's rank is its slot.
     const double inv = P->inv_cell;
     const double cx = floor(__dmul_rn((double)pi.x, inv)), cy = floor(__dmul_rn((double)pi.y, inv)),
                  cz = floor(__dmul_rn((double)pi.z, inv));
     const float R = H * (1.0f + VSKIN), R2 = R * R;
-    uint32_t* __restrict__ lst = v.nbr + f;
+    uint32_t* __restrict__ lst = v.nbr + r;
     const unsigned gmask = 0xFu << ((threadIdx.x & 31) & ~(unsigned)(GLF - 1));
     const unsigned lt = gmask & ((1u << (threadIdx.x & 31)) - 1u);  // group lanes below this one
     auto place = [&](bool kp, uint32_t e) {
       const unsigned bal = __ballot_sync(gmask, kp);
       if (kp) {
         const uint32_t c = lcount + (uint32_t)__popc(bal & lt);
-        if (c < NLT) lst[(size_t)c * FS] = __ldg(&v.entries[e]);
+        if (c < NLT) lst[(size_t)c * NS] = e;
       }
       lcount += (uint32_t)__popc(bal);
     };
+    const int g = (int)threadIdx.x / GLF;
     const uint32_t run = walk_tables<0, GLF>(v, ch, lane, act, g);
     uint32_t k = 0, next = s_walk_off[g][1], base = s_walk_base[g][0];
     for (uint32_t c0 = 0; c0 < run; c0 += GLF) {  // the same trip count for the group's lanes
@@ -220,13 +320,13 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
     });
   }
   if (listed) {  // lane l reads entries l, l + GLF, ...
-    const uint32_t n = v.ncount[f];
-    const uint32_t* __restrict__ lst = v.nbr + f;
-    const float4* __restrict__ pos = v.pos;
+    const uint32_t n = v.ncount[r];
+    const uint32_t* __restrict__ lst = v.nbr + r;
+    const float4* __restrict__ epos = v.epos;
     for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[(size_t)c * FS]);
-      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * FS]) : j0;
-      const float4 p0 = pos[j0], p1 = pos[j1];
+      const uint32_t j0 = __ldg(&lst[(size_t)c * NS]);
+      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * NS]) : j0;
+      const float4 p0 = epos[j0], p1 = epos[j1];
       float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
       float d2 = dot3(ex, ey, ez, ex, ey, ez);
       float q = 1.0f - approx_sqrt(d2) * invH;
@@ -245,17 +345,19 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
   rhoNear = lane_sum<GLF>(rhoNear);
   // a particle whose buckets coincide walks whatever the lists hold: it does
   // not count towards a rebuild
-  if (!rebuild) vl_count_walkers(v, walks && !(pf & PF_DUP), lane);
+  if (!rebuild && P->use_lists) vl_count_walkers(v, walks && !(pf & PF_DUP), lane);
   if (act && lane == 0) {
     const float2 d = make_float2(rho, rhoNear);
     v.density[i] = d;
     v.sdens[myslot] = d;
+    v.edens[r] = d;
     uint32_t npf = pf;
     bool use = listed;
     if (rebuild) {
       const uint32_t cnt = lcount;
-      v.ncount[f] = cnt;
-      v.xlist[f] = pi;
+      v.ncount[r] = cnt;
+      v.xlist[r] = pi;
+      v.epos[r] = pi;
       npf = (cnt > NLT) ? (npf & ~PF_LOK) : (npf | PF_LOK);
       // the fresh list holds exactly this substep's pairs when complete and
       // no two of the 27 buckets coincide: the displacement pass reads it
@@ -268,22 +370,23 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
 
 // fluidDisp (src/gpu/wgsl.js:281-316) over the same pairs as the density
 // pass; with APPLY also applyDeltaFluid (src/gpu/wgsl.js:318-323) into the
-// particle's slot copy sfp (pos[i] is left for the bounds pass to write, so
-// the list reads of pos stay on the pre-displacement positions).
+// particle's slot copy sfp (pos[i] is left for the bounds pass to write).
 template <bool APPLY>
 __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const unsigned FULL = 0xffffffffu;
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GLF - 1);
-  uint32_t myslot, i;
+  const uint32_t r = t / GLF;
+  const bool slots = !P->use_lists;
+  uint32_t i, myslot;
   bool act;
-  slot_group(v, t, myslot, i, act);
+  vl_group(v, r, slots, i, myslot, act);
   if (!__any_sync(FULL, act)) return;
   const bool listed = act && (v.pfl[i] & PF_LIST);
   const bool walks = act && !listed;
   const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
-  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const float2 di = act ? v.sdens[myslot] : make_float2(0.f, 0.f);
+  const float4 pi = act ? (slots ? v.spos[myslot] : v.epos[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float2 di = act ? (slots ? v.sdens[myslot] : v.edens[r]) : make_float2(0.f, 0.f);
   const float maxPair = 0.05f * H;
   const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
   const float Pi = k * (di.x - rho0);
@@ -317,17 +420,16 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
                          });
   }
   if (listed) {  // lane l reads entries l, l + GLF, ...
-    const uint32_t FS = (uint32_t)v.F;
-    const uint32_t f = i - (uint32_t)v.S;
-    const uint32_t n = v.ncount[f];
-    const uint32_t* __restrict__ lst = v.nbr + f;
-    const float4* __restrict__ pos = v.pos;
-    const float2* __restrict__ dens = v.density;
+    const uint32_t NS = (uint32_t)v.N;
+    const uint32_t n = v.ncount[r];
+    const uint32_t* __restrict__ lst = v.nbr + r;
+    const float4* __restrict__ epos = v.epos;
+    const float2* __restrict__ edens = v.edens;
     for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[(size_t)c * FS]);
-      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * FS]) : j0;
-      const float4 p0 = pos[j0], p1 = pos[j1];
-      const float2 d0 = dens[j0], d1 = dens[j1];
+      const uint32_t j0 = __ldg(&lst[(size_t)c * NS]);
+      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * NS]) : j0;
+      const float4 p0 = epos[j0], p1 = epos[j1];
+      const float2 d0 = edens[j0], d1 = edens[j1];
       pair(p0, d0);
       if (c + GLF < n) pair(p1, d1);
     }
@@ -351,48 +453,7 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
     v.delta[i] = make_float4(sx, sy, sz, 1.0f);
 }
 
-// Records, for the xsph pass, how far fluid particle i (at slot sl) has moved
-// since its list was built (smove, and above VMOVE_REC * the allowance its
-// grid bucket's bmove and the scene's SCR_XMOVE), and whether its final cell
-// differs from its grid-time cell o (returned; then PF_DUPF is tested for the
-// new cell). Called by the bounds pass for every active fluid particle.
-__device__ __forceinline__ bool vl_record(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t sl,
-                                          const float4& o, const float4& p) {
-  const unsigned am = __activemask();  // the lanes that reach the warp reduction below
-  const float m = vl_dist(p, v.xlist[i - v.S]);
-  v.smove[sl] = m;
-  const bool rec = m > VMOVE_REC * vl_allowance(P);
-  if (rec) atomicMax(&v.bmove[v.cell[i]], __float_as_uint(m));
-  const uint32_t wm = __reduce_max_sync(am, rec ? __float_as_uint(m) : 0u);
-  if (wm != 0u && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&v.scratch[SCR_XMOVE], wm);
-  const double inv = P->inv_cell;
-  const bool same = floor(__dmul_rn((double)o.x, inv)) == floor(__dmul_rn((double)p.x, inv)) &&
-                    floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
-                    floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
-  const uint32_t pf = v.pfl[i];
-  bool dupf = (pf & PF_DUP) != 0u;
-  if (!same) {
-    CellHash ch;
-    ch.init(p.x, p.y, p.z, inv);
-    dupf = buckets_coincide(ch, (uint32_t)v.T - 1u);
-  }
-  v.pfl[i] = dupf ? (pf | PF_DUPF) : (pf & ~PF_DUPF);
-  return !same;
-}
-
-// Grid-time movement since the list build, recorded by the rank fix-up for
-// the density pass's test (skipped at a rebuild: the lists are rebuilt from
-// the positions the density pass sees).
-__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h) {
-  const unsigned am = __activemask();  // the lanes that reach the warp reduction below
-  const float m = vl_dist(v.pos[i], v.xlist[i - v.S]);
-  const bool rec = m > VMOVE_REC * vl_allowance(P);
-  if (rec) atomicMax(&v.bmove[h], __float_as_uint(m));
-  const uint32_t wm = __reduce_max_sync(am, rec ? __float_as_uint(m) : 0u);
-  if (wm != 0u && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&v.scratch[SCR_XMOVE], wm);
-}
-
-// j's grid-time bucket is one of the 27 around the cell of p.
+// Particle j's grid-time bucket is one of the 27 around the cell of p.
 static __device__ __noinline__ bool vl_member(const SimView& v, const DevParams* __restrict__ P, const float4& p,
                                               uint32_t j) {
   CellHash ch;
@@ -411,24 +472,30 @@ static __device__ __noinline__ bool vl_member(const SimView& v, const DevParams*
 // xsph (src/gpu/wgsl.js:745-771) at the final positions; with APPLY the
 // blended velocity goes to vel[i] (xsphApply, src/gpu/wgsl.js:773-778), the
 // neighbours' velocities being read from the copies the velocity pass wrote
-// (svel by slot for walks, ivel by index for lists).
+// (svel by slot for walks, evel by rank for lists).
 template <bool APPLY>
 __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const unsigned FULL = 0xffffffffu;
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GLF - 1);
-  uint32_t myslot, i;
+  const uint32_t r = t / GLF;
+  const bool slots = !P->use_lists;
+  uint32_t i, myslot;
   bool fluid;
-  slot_group(v, t, myslot, i, fluid);
+  vl_group(v, r, slots, i, myslot, fluid);
   const bool act = fluid && (v.flags[i] & F_ACTIVE);
   if (!__any_sync(FULL, act)) return;
-  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
+  // the bounds pass wrote the final position to both copies
+  const float4 pi = act ? (slots ? v.spos[myslot] : v.epos[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
   const float H = P->fluid_h, H2 = H * H;
   const float allow = vl_allowance(P), rec = VMOVE_REC * allow;
   const uint32_t pf = act ? v.pfl[i] : 0u;
-  const float mv = act ? v.smove[myslot] : 0.f;
-  const bool cand = act && P->use_lists && (pf & (PF_LOK | PF_DUPF)) == PF_LOK && mv + rec <= allow;
-  const bool quick = cand && mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
+  const float mv = (act && !slots) ? v.smove[r] : 0.f;
+  const bool cand = act && !slots && (pf & (PF_LOK | PF_DUPF)) == PF_LOK && mv + rec <= allow;
+  // a particle that kept its cell reads its grid bucket's fast mark; one that
+  // changed cell takes the per-bucket test
+  const bool quick = cand && !(pf & PF_MOVED) && v.bfast[v.cell[i]] == 0u &&
+                     mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
   const bool need = cand && !quick;
   bool listed = quick;
   CellHash ch;
@@ -454,25 +521,26 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
                          });
   }
   if (listed) {  // lane l reads entries l, l + GLF, ...
-    const uint32_t FS = (uint32_t)v.F;
-    const uint32_t f = i - (uint32_t)v.S;
-    const uint32_t n = v.ncount[f];
-    const uint32_t* __restrict__ lst = v.nbr + f;
-    const float4* __restrict__ pos = v.pos;
-    const float4* __restrict__ ivel = v.ivel;
+    const uint32_t NS = (uint32_t)v.N;
+    const uint32_t n = v.ncount[r];
+    const uint32_t* __restrict__ lst = v.nbr + r;
+    const float4* __restrict__ epos = v.epos;
+    const float4* __restrict__ evel = v.evel;
     for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[(size_t)c * FS]);
-      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * FS]) : j0;
-      const float4 p0 = pos[j0], p1 = pos[j1];
-      const float4 u0 = ivel[j0], u1 = ivel[j1];
+      const uint32_t j0 = __ldg(&lst[(size_t)c * NS]);
+      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * NS]) : j0;
+      const float4 p0 = epos[j0], p1 = epos[j1];
+      const float4 u0 = evel[j0], u1 = evel[j1];
       float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
       bool in = dot3(ex, ey, ez, ex, ey, ez) < H2;
-      if (in && u0.w != 0.f) in = vl_member(v, P, pi, j0);  // j0 changed cell after the grid build
+      // a neighbour that changed cell after the grid build counts when its
+      // grid bucket is one of this particle's 27
+      if (in && u0.w != 0.f) in = vl_member(v, P, pi, v.ep[j0]);
       sx = sx + (in ? u0.x : 0.f); sy = sy + (in ? u0.y : 0.f); sz = sz + (in ? u0.z : 0.f);
       m = m + (in ? 1.0f : 0.f);
       ex = p1.x - pi.x; ey = p1.y - pi.y; ez = p1.z - pi.z;
       in = (c + GLF < n) && dot3(ex, ey, ez, ex, ey, ez) < H2;
-      if (in && u1.w != 0.f) in = vl_member(v, P, pi, j1);
+      if (in && u1.w != 0.f) in = vl_member(v, P, pi, v.ep[j1]);
       sx = sx + (in ? u1.x : 0.f); sy = sy + (in ? u1.y : 0.f); sz = sz + (in ? u1.z : 0.f);
       m = m + (in ? 1.0f : 0.f);
     }
@@ -481,7 +549,7 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
   sy = lane_sum<GLF>(sy);
   sz = lane_sum<GLF>(sz);
   m = lane_sum<GLF>(m);
-  vl_count_walkers(v, walks && !(pf & PF_DUPF), lane);
+  if (!slots) vl_count_walkers(v, walks && !(pf & PF_DUPF), lane);
   if (act && lane == 0) {
     const float4 vi = v.vel[i];
     float vx = vi.x, vy = vi.y, vz = vi.z;
