@@ -226,6 +226,12 @@ int launch_substep(upbd_sim* s, int last) {
   }
   if (last < UPBD_PASS_DENSITY) return UPBD_OK;
   const long long fl = (long long)v.N * GLF;  // lane-parallel fluid gathers over the slots
+#ifndef UPBD_PARITY_BUILD
+  // a rebuild substep's density (lists, rank order) in a launch of its own,
+  // so the list launch keeps few registers; each returns on the other's substeps
+  PROF(s, K_DENSITY, k_density_rebuild<<<blocks_for(fl), 256, 0, st>>>(v, P));
+  L++;
+#endif
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_DISP) return UPBD_OK;

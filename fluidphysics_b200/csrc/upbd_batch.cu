@@ -125,6 +125,11 @@ __global__ void __launch_bounds__(256, 6) kb_density(BatchArgs a) {
   batch_loop<D_FGL, false, true>(a, UPBD_BODY { b_density_vl(v, P, vb); });
 #endif
 }
+#ifndef UPBD_PARITY_BUILD
+__global__ void __launch_bounds__(256) kb_density_rebuild(BatchArgs a) {
+  batch_loop<D_FGL, false, true>(a, UPBD_BODY { b_density_rebuild_vl(v, P, vb); });
+}
+#endif
 template <bool APPLY>
 __global__ void __launch_bounds__(256) kb_disp(BatchArgs a) {
 #ifdef UPBD_PARITY_BUILD
@@ -448,6 +453,9 @@ int launch_batch_frame(upbd_batch* b, int nsub, bool visc) {
     BLAUNCH(b, K_SCAN, kb_scan<<<G, SCAN_THREADS, 0, st>>>(a));
     BLAUNCH(b, K_SCATTER, kb_scatter<<<G, BT, 0, st>>>(a));
     BLAUNCH(b, K_RANKFIX, kb_rankfix<<<G, BT, 0, st>>>(a));
+#ifndef UPBD_PARITY_BUILD
+    BLAUNCH(b, K_DENSITY, kb_density_rebuild<<<G, BT, 0, st>>>(a));  // returns at once without a rebuild
+#endif
     BLAUNCH(b, K_DENSITY, kb_density<<<G, BT, 0, st>>>(a));
     if (fold)  // the displacement pass applies the fluid's move (b_disp<true>)
       BLAUNCH(b, K_DISP, kb_disp<true><<<G, BT, 0, st>>>(a));

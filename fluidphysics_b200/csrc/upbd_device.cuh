@@ -141,6 +141,10 @@ struct SimView {
   // the scan every substep).
   uint32_t* ep;
   uint32_t* erank;
+  // per rank {particle, slot, grid bucket, state bits}: written by the rank
+  // fix-up (a rebuild: the density pass), the state bits updated by the
+  // density and bounds passes; the gathers start from it with one load
+  uint4* erec;
   float4* xlist;
   float4* epos;
   float2* edens;
@@ -284,9 +288,11 @@ constexpr uint32_t PF_DUPF = 2u;   // the same for the cell at xsph time
 constexpr uint32_t PF_LOK = 4u;    // the list is complete (it did not overflow at the rebuild)
 constexpr uint32_t PF_LIST = 8u;   // this substep's density and displacement read the list
 constexpr uint32_t PF_MOVED = 16u; // the particle changed cell after this substep's grid build
+constexpr uint32_t PF_CULLED = 32u; // (rank record only) culled by this substep's bounds pass
 // A rebuild follows a substep whose density and xsph passes walked, for want
-// of a usable list, for more than F / VWALK_DIV particles.
-constexpr uint32_t VWALK_DIV = 512u;
+// of a usable list, for more than F / VWALK_DIV particles (walkers sit
+// together in rank order, so a few hundred cost little).
+constexpr uint32_t VWALK_DIV = 64u;
 
 template <int G = GL>
 __device__ __forceinline__ float lane_sum(float x) {

@@ -66,6 +66,13 @@ __global__ void __launch_bounds__(256) k_scatter(SimView v) { b_scatter(v, block
 __global__ void __launch_bounds__(256) k_rankfix(SimView v, const DevParams* __restrict__ P) {
   b_rankfix(v, P, blockIdx.x);
 }
+#ifndef UPBD_PARITY_BUILD
+// Product build: a rebuild substep's density pass (returns at once on the
+// others, where k_density runs over the lists instead).
+__global__ void __launch_bounds__(256) k_density_rebuild(SimView v, const DevParams* __restrict__ P) {
+  b_density_rebuild_vl(v, P, blockIdx.x);
+}
+#endif
 // The fluid gathers: the bucket walks in the parity build (the oracle's
 // summation order), lists kept across substeps in the product build.
 __global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __restrict__ P) {
@@ -295,11 +302,13 @@ __global__ void k_list_census(SimView v) {
   const int i = v.S + (int)UPBD_TID;
   uint32_t listed = 0, complete = 0, len = 0;
   if (i < v.N && (v.flags[i] & F_ACTIVE) && v.pfl) {
-    const uint32_t pf = v.pfl[i];
     const uint32_t r = v.erank[i];
-    listed = (pf & PF_LIST) ? 1u : 0u;
-    complete = (pf & PF_LOK) ? 1u : 0u;
-    len = (r < (uint32_t)v.N) ? v.ncount[r] : 0u;
+    if (r < (uint32_t)v.N) {
+      const uint32_t pf = v.erec[r].w;
+      listed = (pf & PF_LIST) ? 1u : 0u;
+      complete = (pf & PF_LOK) ? 1u : 0u;
+      len = v.ncount[r];
+    }
   }
   listed = __reduce_add_sync(0xffffffffu, listed);
   complete = __reduce_add_sync(0xffffffffu, complete);

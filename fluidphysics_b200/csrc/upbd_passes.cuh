@@ -216,7 +216,8 @@ __device__ __forceinline__ void b_scatter(const SimView& v, uint32_t vb) {
 
 #ifndef UPBD_PARITY_BUILD
 // grid-time movement since the list build (upbd_vlist.cuh)
-__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h);
+__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h,
+                                               uint32_t slot);
 #endif
 
 // Deterministic membership: particle i goes to start[h] + #{j in bucket : j > i},
@@ -241,7 +242,7 @@ __device__ __forceinline__ void b_rankfix(const SimView& v, const DevParams* __r
     v.fend[h] = e - solids;  // every member writes the same value
   }
 #ifndef UPBD_PARITY_BUILD
-  if (v.pfl && i >= v.S && P->use_lists && v.scratch[SCR_REBUILD] == 0u) vl_record_grid(v, P, i, h);
+  if (v.pfl && i >= v.S && P->use_lists && v.scratch[SCR_REBUILD] == 0u) vl_record_grid(v, P, i, h, s + rank);
 #endif
 }
 
@@ -1020,7 +1021,7 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   const float moved = 0.f;
 #else
   const uint32_t erk = (!iSolid && P->use_lists) ? v.erank[i] : NO_RANK;
-  const float moved = (erk != NO_RANK && vl_record(v, P, i, erk, o, p)) ? 1.f : 0.f;
+  const float moved = (erk != NO_RANK && vl_record(v, P, i, erk, o, p, culled)) ? 1.f : 0.f;
   if (culled) atomicOr(&v.scratch[SCR_DIRTY], 1u);  // the next substep rebuilds the lists
 #endif
   v.spos[sl] = p;

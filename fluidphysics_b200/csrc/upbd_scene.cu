@@ -196,6 +196,7 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.bmove = cv.take<uint32_t>(v.T);
   L.ep = cv.take<uint32_t>(v.N);
   L.erank = cv.take<uint32_t>(v.N);
+  L.erec = cv.take<uint4>(v.N);
   L.xlist = cv.take<float4>(v.N);
   L.epos = cv.take<float4>(v.N);
   L.edens = cv.take<float2>(v.N);
@@ -245,6 +246,7 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.bmove = (uint32_t*)(base + L.bmove);
   v.ep = (uint32_t*)(base + L.ep);
   v.erank = (uint32_t*)(base + L.erank);
+  v.erec = (uint4*)(base + L.erec);
   v.xlist = (float4*)(base + L.xlist);
   v.epos = (float4*)(base + L.epos);
   v.edens = (float2*)(base + L.edens);

@@ -102,9 +102,10 @@ __device__ __forceinline__ void vl_note_move(const SimView& v, const DevParams* 
 }
 
 // Grid-time record by the rank fix-up (not at a rebuild, when the density
-// pass itself rewrites the rank copies): the position copy for the density
+// rebuild writes them): the rank record, the position copy for the density
 // and displacement passes, and the movement since the list build.
-__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h) {
+__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h,
+                                               uint32_t slot) {
   const unsigned am = __activemask();  // the lanes that reach the warp reduction below
   const uint32_t r = v.erank[i];
   float m = 0.f;
@@ -112,6 +113,7 @@ __device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams
   if (r != NO_RANK) {
     p = v.pos[i];
     v.epos[r] = p;
+    v.erec[r] = make_uint4((uint32_t)i, slot, h, v.pfl[i] & (PF_DUP | PF_LOK));
     m = vl_dist(p, v.xlist[r]);
   }
   vl_note_move(v, P, am, m, h, p);
@@ -119,11 +121,11 @@ __device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams
 
 // Final-time record by the bounds pass for fluid particle i of rank r: its
 // final position copy, how far it moved since its list was built (smove[r]
-// and the bucket / scene records), and whether its final cell differs from
-// its grid-time cell o (returned, and PF_MOVED; then PF_DUPF is tested for
-// the new cell).
+// and the bucket / scene records), whether its final cell differs from its
+// grid-time cell o (returned; PF_MOVED, and then PF_DUPF is tested for the
+// new cell) and whether it was culled (PF_CULLED), into the rank record.
 __device__ __forceinline__ bool vl_record(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t r,
-                                          const float4& o, const float4& p) {
+                                          const float4& o, const float4& p, bool culled) {
   const unsigned am = __activemask();  // the lanes that reach the warp reduction below
   v.epos[r] = p;
   const float m = vl_dist(p, v.xlist[r]);
@@ -133,16 +135,16 @@ __device__ __forceinline__ bool vl_record(const SimView& v, const DevParams* __r
   const bool same = floor(__dmul_rn((double)o.x, inv)) == floor(__dmul_rn((double)p.x, inv)) &&
                     floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
                     floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
-  const uint32_t pf = v.pfl[i];
+  const uint32_t pf = v.erec[r].w;
   bool dupf = (pf & PF_DUP) != 0u;
   if (!same) {
     CellHash ch;
     ch.init(p.x, p.y, p.z, inv);
     dupf = buckets_coincide(ch, (uint32_t)v.T - 1u);
   }
-  uint32_t npf = dupf ? (pf | PF_DUPF) : (pf & ~PF_DUPF);
-  npf = same ? (npf & ~PF_MOVED) : (npf | PF_MOVED);
-  v.pfl[i] = npf;
+  uint32_t npf = pf & ~(PF_DUPF | PF_MOVED | PF_CULLED);
+  npf |= (dupf ? PF_DUPF : 0u) | (same ? 0u : PF_MOVED) | (culled ? PF_CULLED : 0u);
+  v.erec[r].w = npf;
   return !same;
 }
 
@@ -173,33 +175,206 @@ __device__ __forceinline__ void vl_group(const SimView& v, uint32_t r, bool slot
   fluid = i != NO_RANK && i >= (uint32_t)v.S;
 }
 
-// fluidDensity (src/gpu/wgsl.js:254-279); a rebuild also sets the rank
-// order to this substep's grid order and writes the lists.
-__device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
+// Density of one group over its list (lane l: entries l, l + GLF, ...,
+// four entries' loads in flight).
+__device__ __forceinline__ void vl_density_list(const SimView& v, uint32_t r, int lane, const float4& pi, float H2,
+                                                float invH, float& rho, float& rhoNear) {
+  const uint32_t NS = (uint32_t)v.N;
+  const uint32_t n = v.ncount[r];
+  const uint32_t* __restrict__ lst = v.nbr + r;
+  const float4* __restrict__ epos = v.epos;
+  for (uint32_t c = (uint32_t)lane; c < n; c += 4 * GLF) {
+    uint32_t j[4];
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+      const uint32_t cw = c + (uint32_t)(w * GLF);
+      j[w] = (cw < n) ? __ldg(&lst[(size_t)cw * NS]) : NO_RANK;
+    }
+    float4 pj[4];
+#pragma unroll
+    for (int w = 0; w < 4; w++) pj[w] = epos[(j[w] != NO_RANK) ? j[w] : j[0]];
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+      const float ex = pj[w].x - pi.x, ey = pj[w].y - pi.y, ez = pj[w].z - pi.z;
+      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      const float q = 1.0f - approx_sqrt(d2) * invH;
+      const float qq = (d2 < H2 && j[w] != NO_RANK) ? q * q : 0.0f;
+      rho = rho + qq;
+      rhoNear = rhoNear + qq * q;
+    }
+  }
+}
+
+// fluidDensity (src/gpu/wgsl.js:254-279) at a rebuild substep: sets the rank
+// order to this substep's grid order and writes the lists (the list kernel
+// below has nothing to do then). Returns at once on other substeps.
+__device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const DevParams* __restrict__ P,
+                                                     uint32_t vb) {
   const unsigned FULL = 0xffffffffu;
-  const bool rebuild = v.scratch[SCR_REBUILD] != 0u;  // one value for the whole scene
-  if (rebuild && vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
+  if (v.scratch[SCR_REBUILD] == 0u) return;  // one value for the whole scene
+  if (vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
   const uint32_t t = UPBD_VTID;
   const int lane = threadIdx.x & (GLF - 1);
-  const uint32_t r = t / GLF;  // this group's rank
-  const bool slots = rebuild || !P->use_lists;
+  const uint32_t r = t / GLF;  // this group's rank = its slot
   uint32_t i, myslot;
   bool act;
-  vl_group(v, r, slots, i, myslot, act);
-  if (rebuild && lane == 0 && r < (uint32_t)v.N) {  // the new rank order
+  vl_group(v, r, true, i, myslot, act);
+  if (lane == 0 && r < (uint32_t)v.N) {  // the new rank order
     v.ep[r] = i;
     if (i != NO_RANK) v.erank[i] = r;
   }
   if (!__any_sync(FULL, act)) return;
-  const float4 pi = act ? (slots ? v.spos[myslot] : v.epos[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
   const uint32_t NS = (uint32_t)v.N;
   const uint32_t pf = act ? v.pfl[i] : 0u;
+  const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
+  CellHash ch;
+  group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
+  float rho = 0.f, rhoNear = 0.f;
+  const float4* __restrict__ spos = v.spos;
+  uint32_t lcount = 0;
+  // The reference's density over the 27 cells (every bucket visit counted,
+  // coinciding buckets included) and, for the list, every fluid candidate
+  // within R met at the visit of its own cell (so a bucket met through two
+  // cells lists it once); then the cells past the 27 that R reaches. The
+  // group's lanes step together and place their entries by a ballot, so the
+  // list holds the candidates in walk order (deterministic sums). At a
+  // rebuild a candidate's rank is its slot.
+  const double inv = P->inv_cell;
+  const double cx = floor(__dmul_rn((double)pi.x, inv)), cy = floor(__dmul_rn((double)pi.y, inv)),
+               cz = floor(__dmul_rn((double)pi.z, inv));
+  const float R = H * (1.0f + VSKIN), R2 = R * R;
+  uint32_t* __restrict__ lst = v.nbr + r;
+  const unsigned gmask = 0xFu << ((threadIdx.x & 31) & ~(unsigned)(GLF - 1));
+  const unsigned lt = gmask & ((1u << (threadIdx.x & 31)) - 1u);  // group lanes below this one
+  auto place = [&](bool kp, uint32_t e) {
+    const unsigned bal = __ballot_sync(gmask, kp);
+    if (kp) {
+      const uint32_t c = lcount + (uint32_t)__popc(bal & lt);
+      if (c < NLT) lst[(size_t)c * NS] = e;
+    }
+    lcount += (uint32_t)__popc(bal);
+  };
+  const int g = (int)threadIdx.x / GLF;
+  const uint32_t run = walk_tables<0, GLF>(v, ch, lane, act, g);
+  uint32_t k = 0, next = s_walk_off[g][1], base = s_walk_base[g][0];
+  for (uint32_t c0 = 0; c0 < run; c0 += GLF) {  // the same trip count for the group's lanes
+    const uint32_t c = c0 + (uint32_t)lane;
+    bool kp = false;
+    uint32_t e = 0;
+    if (c < run) {
+      while (c >= next) {
+        k++;
+        next = s_walk_off[g][k + 1];
+        base = s_walk_base[g][k];
+      }
+      e = base + c;
+      const float4 pj = spos[e];
+      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+      const bool in = (e != myslot) && (d2 < H2);
+      const float q = 1.0f - approx_sqrt(d2) * invH;
+      const float qq = in ? q * q : 0.0f;
+      rho = rho + qq;
+      rhoNear = rhoNear + qq * q;
+      if (e != myslot && d2 < R2) {
+        const int a = (int)k / 9 - 1, b = ((int)k / 3) % 3 - 1, cc = (int)k % 3 - 1;
+        kp = vl_in_cell(pj, inv, cx + a, cy + b, cz + cc);
+      }
+    }
+    place(kp, e);
+  }
+  __syncwarp();  // the walk tables are free again
+  if (act) {
+    // reach of R past the 27 cells, in cells (R is below two cells)
+    const double ext = (double)R * inv - 1.0 + 1e-3, rc2 = ((double)R * inv) * ((double)R * inv) * 1.0001;
+    const double fx = __dmul_rn((double)pi.x, inv) - cx, fy = __dmul_rn((double)pi.y, inv) - cy,
+                 fz = __dmul_rn((double)pi.z, inv) - cz;
+    const int lox = (fx < ext) ? -2 : -1, hix = (1.0 - fx < ext) ? 2 : 1;
+    const int loy = (fy < ext) ? -2 : -1, hiy = (1.0 - fy < ext) ? 2 : 1;
+    const int loz = (fz < ext) ? -2 : -1, hiz = (1.0 - fz < ext) ? 2 : 1;
+    if (lox < -1 || hix > 1 || loy < -1 || hiy > 1 || loz < -1 || hiz > 1) {
+      const int32_t xm2 = js_toint32(__dmul_rn(__dadd_rn(cx, -2.0), 92837111.0));
+      const int32_t xp2 = js_toint32(__dmul_rn(__dadd_rn(cx, 2.0), 92837111.0));
+      const int32_t ym2 = js_toint32(__dmul_rn(__dadd_rn(cy, -2.0), 689287499.0));
+      const int32_t yp2 = js_toint32(__dmul_rn(__dadd_rn(cy, 2.0), 689287499.0));
+      const int32_t zm2 = js_toint32(__dmul_rn(__dadd_rn(cz, -2.0), 283923481.0));
+      const int32_t zp2 = js_toint32(__dmul_rn(__dadd_rn(cz, 2.0), 283923481.0));
+      const uint32_t mask = (uint32_t)v.T - 1u;
+      for (int a = lox; a <= hix; a++)
+        for (int b = loy; b <= hiy; b++)
+          for (int c = loz; c <= hiz; c++) {
+            if (a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1) continue;  // one of the 27
+            // distance (in cells) from the particle to the cell's box
+            const double gx = (a < 0) ? fx + (double)(-a - 1) : ((a > 0) ? (1.0 - fx) + (double)(a - 1) : 0.0);
+            const double gy = (b < 0) ? fy + (double)(-b - 1) : ((b > 0) ? (1.0 - fy) + (double)(b - 1) : 0.0);
+            const double gz = (c < 0) ? fz + (double)(-c - 1) : ((c > 0) ? (1.0 - fz) + (double)(c - 1) : 0.0);
+            if (gx * gx + gy * gy + gz * gz > rc2) continue;
+            const uint32_t h = (uint32_t)(vl_sel(a, xm2, ch.hx[0], ch.hx[1], ch.hx[2], xp2) ^
+                                          vl_sel(b, ym2, ch.hy[0], ch.hy[1], ch.hy[2], yp2) ^
+                                          vl_sel(c, zm2, ch.hz[0], ch.hz[1], ch.hz[2], zp2)) & mask;
+            const uint32_t s0 = __ldg(&v.start[h]), s1 = __ldg(&v.fend[h]);
+            for (uint32_t e0 = s0; e0 < s1; e0 += GLF) {  // the same trip count for the group's lanes
+              const uint32_t e = e0 + (uint32_t)lane;
+              bool kp = false;
+              if (e < s1) {
+                const float4 pj = spos[e];
+                const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+                kp = dot3(ex, ey, ez, ex, ey, ez) < R2 &&
+                     vl_in_cell(pj, inv, cx + (double)a, cy + (double)b, cz + (double)c);
+              }
+              place(kp, e);
+            }
+          }
+    }
+  }
+  rho = lane_sum<GLF>(rho);
+  rhoNear = lane_sum<GLF>(rhoNear);
+  if (act && lane == 0) {
+    const float2 d = make_float2(rho, rhoNear);
+    v.density[i] = d;
+    v.sdens[myslot] = d;
+    v.edens[r] = d;
+    v.ncount[r] = lcount;
+    v.xlist[r] = pi;
+    v.epos[r] = pi;
+    const bool ok = lcount <= NLT;
+    const uint32_t npf = ok ? (pf | PF_LOK) : (pf & ~PF_LOK);
+    v.pfl[i] = npf;
+    // the fresh list holds exactly this substep's pairs when complete and no
+    // two of the 27 buckets coincide: the displacement pass reads it
+    const uint32_t rpf = (npf & (PF_DUP | PF_LOK)) | ((ok && !(pf & PF_DUP)) ? PF_LIST : 0u);
+    v.erec[r] = make_uint4(i, myslot, v.cell[i], rpf);
+  }
+}
+
+// fluidDensity (src/gpu/wgsl.js:254-279) on the substeps without a rebuild:
+// each group reads its list when the movement test allows and walks the 27
+// buckets otherwise (every group walks when lists are off).
+__device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
+  const unsigned FULL = 0xffffffffu;
+  if (v.scratch[SCR_REBUILD] != 0u) return;  // the rebuild kernel did this substep's density
+  const uint32_t t = UPBD_VTID;
+  const int lane = threadIdx.x & (GLF - 1);
+  const uint32_t r = t / GLF;  // this group's rank (or slot, lists off)
+  const bool slots = !P->use_lists;
+  uint32_t i, myslot, h = 0, pf = 0;
+  bool act;
+  if (slots) {
+    vl_group(v, r, true, i, myslot, act);
+  } else {
+    const uint4 rc = (r < (uint32_t)v.N) ? v.erec[r] : make_uint4(NO_RANK, 0u, 0u, 0u);
+    i = rc.x; myslot = rc.y; h = rc.z; pf = rc.w;
+    act = i != NO_RANK && i >= (uint32_t)v.S && r < (uint32_t)v.N && v.ep[r] == i;
+  }
+  if (!__any_sync(FULL, act)) return;
+  const float4 pi = act ? (slots ? v.spos[myslot] : v.epos[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
   const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
   const float allow = vl_allowance(P), rec = VMOVE_REC * allow;
   const bool cand = act && !slots && (pf & (PF_LOK | PF_DUP)) == PF_LOK;
   const float mv = cand ? vl_dist(pi, v.xlist[r]) : 0.f;
   const bool quick = cand && mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow &&
-                     v.bfast[v.cell[i]] == 0u;
+                     v.bfast[h] == 0u;
   const bool need = cand && !quick && mv + rec <= allow;
   bool listed = quick;
   CellHash ch;
@@ -210,105 +385,8 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
   }
   const bool walks = act && !listed;
   float rho = 0.f, rhoNear = 0.f;
-  const float4* __restrict__ spos = v.spos;
-  uint32_t lcount = 0;  // list length (rebuild)
-  if (rebuild) {
-    // The reference's density over the 27 cells (every bucket visit counted,
-    // coinciding buckets included) and, for the list, every fluid candidate
-    // within R met at the visit of its own cell (so a bucket met through two
-    // cells lists it once); then the cells past the 27 that R reaches. The
-    // group's lanes step together and place their entries by a ballot, so the
-    // list holds the candidates in walk order (deterministic sums). At a
-    // rebuild a candidate's rank is its slot.
-    const double inv = P->inv_cell;
-    const double cx = floor(__dmul_rn((double)pi.x, inv)), cy = floor(__dmul_rn((double)pi.y, inv)),
-                 cz = floor(__dmul_rn((double)pi.z, inv));
-    const float R = H * (1.0f + VSKIN), R2 = R * R;
-    uint32_t* __restrict__ lst = v.nbr + r;
-    const unsigned gmask = 0xFu << ((threadIdx.x & 31) & ~(unsigned)(GLF - 1));
-    const unsigned lt = gmask & ((1u << (threadIdx.x & 31)) - 1u);  // group lanes below this one
-    auto place = [&](bool kp, uint32_t e) {
-      const unsigned bal = __ballot_sync(gmask, kp);
-      if (kp) {
-        const uint32_t c = lcount + (uint32_t)__popc(bal & lt);
-        if (c < NLT) lst[(size_t)c * NS] = e;
-      }
-      lcount += (uint32_t)__popc(bal);
-    };
-    const int g = (int)threadIdx.x / GLF;
-    const uint32_t run = walk_tables<0, GLF>(v, ch, lane, act, g);
-    uint32_t k = 0, next = s_walk_off[g][1], base = s_walk_base[g][0];
-    for (uint32_t c0 = 0; c0 < run; c0 += GLF) {  // the same trip count for the group's lanes
-      const uint32_t c = c0 + (uint32_t)lane;
-      bool kp = false;
-      uint32_t e = 0;
-      if (c < run) {
-        while (c >= next) {
-          k++;
-          next = s_walk_off[g][k + 1];
-          base = s_walk_base[g][k];
-        }
-        e = base + c;
-        const float4 pj = spos[e];
-        const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-        const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-        const bool in = (e != myslot) && (d2 < H2);
-        const float q = 1.0f - approx_sqrt(d2) * invH;
-        const float qq = in ? q * q : 0.0f;
-        rho = rho + qq;
-        rhoNear = rhoNear + qq * q;
-        if (e != myslot && d2 < R2) {
-          const int a = (int)k / 9 - 1, b = ((int)k / 3) % 3 - 1, cc = (int)k % 3 - 1;
-          kp = vl_in_cell(pj, inv, cx + a, cy + b, cz + cc);
-        }
-      }
-      place(kp, e);
-    }
-    __syncwarp();  // the tables are rewritten by the next walk
-    if (act) {
-      // reach of R past the 27 cells, in cells (R is below two cells)
-      const double ext = (double)R * inv - 1.0 + 1e-3, rc2 = ((double)R * inv) * ((double)R * inv) * 1.0001;
-      const double fx = __dmul_rn((double)pi.x, inv) - cx, fy = __dmul_rn((double)pi.y, inv) - cy,
-                   fz = __dmul_rn((double)pi.z, inv) - cz;
-      const int lox = (fx < ext) ? -2 : -1, hix = (1.0 - fx < ext) ? 2 : 1;
-      const int loy = (fy < ext) ? -2 : -1, hiy = (1.0 - fy < ext) ? 2 : 1;
-      const int loz = (fz < ext) ? -2 : -1, hiz = (1.0 - fz < ext) ? 2 : 1;
-      if (lox < -1 || hix > 1 || loy < -1 || hiy > 1 || loz < -1 || hiz > 1) {
-        const int32_t xm2 = js_toint32(__dmul_rn(__dadd_rn(cx, -2.0), 92837111.0));
-        const int32_t xp2 = js_toint32(__dmul_rn(__dadd_rn(cx, 2.0), 92837111.0));
-        const int32_t ym2 = js_toint32(__dmul_rn(__dadd_rn(cy, -2.0), 689287499.0));
-        const int32_t yp2 = js_toint32(__dmul_rn(__dadd_rn(cy, 2.0), 689287499.0));
-        const int32_t zm2 = js_toint32(__dmul_rn(__dadd_rn(cz, -2.0), 283923481.0));
-        const int32_t zp2 = js_toint32(__dmul_rn(__dadd_rn(cz, 2.0), 283923481.0));
-        const uint32_t mask = (uint32_t)v.T - 1u;
-        for (int a = lox; a <= hix; a++)
-          for (int b = loy; b <= hiy; b++)
-            for (int c = loz; c <= hiz; c++) {
-              if (a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1) continue;  // one of the 27
-              // distance (in cells) from the particle to the cell's box
-              const double gx = (a < 0) ? fx + (double)(-a - 1) : ((a > 0) ? (1.0 - fx) + (double)(a - 1) : 0.0);
-              const double gy = (b < 0) ? fy + (double)(-b - 1) : ((b > 0) ? (1.0 - fy) + (double)(b - 1) : 0.0);
-              const double gz = (c < 0) ? fz + (double)(-c - 1) : ((c > 0) ? (1.0 - fz) + (double)(c - 1) : 0.0);
-              if (gx * gx + gy * gy + gz * gz > rc2) continue;
-              const uint32_t h = (uint32_t)(vl_sel(a, xm2, ch.hx[0], ch.hx[1], ch.hx[2], xp2) ^
-                                            vl_sel(b, ym2, ch.hy[0], ch.hy[1], ch.hy[2], yp2) ^
-                                            vl_sel(c, zm2, ch.hz[0], ch.hz[1], ch.hz[2], zp2)) & mask;
-              const uint32_t s0 = __ldg(&v.start[h]), s1 = __ldg(&v.fend[h]);
-              for (uint32_t e0 = s0; e0 < s1; e0 += GLF) {  // the same trip count for the group's lanes
-                const uint32_t e = e0 + (uint32_t)lane;
-                bool kp = false;
-                if (e < s1) {
-                  const float4 pj = spos[e];
-                  const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-                  kp = dot3(ex, ey, ez, ex, ey, ez) < R2 &&
-                       vl_in_cell(pj, inv, cx + (double)a, cy + (double)b, cz + (double)c);
-                }
-                place(kp, e);
-              }
-            }
-      }
-    }
-  } else if (__any_sync(FULL, walks)) {
+  if (__any_sync(FULL, walks)) {
+    const float4* __restrict__ spos = v.spos;
     lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
       const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
       const float d2 = dot3(ex, ey, ez, ex, ey, ez);
@@ -319,52 +397,20 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
       rhoNear = rhoNear + qq * q;
     });
   }
-  if (listed) {  // lane l reads entries l, l + GLF, ...
-    const uint32_t n = v.ncount[r];
-    const uint32_t* __restrict__ lst = v.nbr + r;
-    const float4* __restrict__ epos = v.epos;
-    for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[(size_t)c * NS]);
-      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * NS]) : j0;
-      const float4 p0 = epos[j0], p1 = epos[j1];
-      float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
-      float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      float q = 1.0f - approx_sqrt(d2) * invH;
-      float qq = (d2 < H2) ? q * q : 0.0f;
-      rho = rho + qq;
-      rhoNear = rhoNear + qq * q;
-      ex = p1.x - pi.x; ey = p1.y - pi.y; ez = p1.z - pi.z;
-      d2 = dot3(ex, ey, ez, ex, ey, ez);
-      q = 1.0f - approx_sqrt(d2) * invH;
-      qq = (d2 < H2 && c + GLF < n) ? q * q : 0.0f;
-      rho = rho + qq;
-      rhoNear = rhoNear + qq * q;
-    }
-  }
+  if (listed) vl_density_list(v, r, lane, pi, H2, invH, rho, rhoNear);
   rho = lane_sum<GLF>(rho);
   rhoNear = lane_sum<GLF>(rhoNear);
   // a particle whose buckets coincide walks whatever the lists hold: it does
   // not count towards a rebuild
-  if (!rebuild && P->use_lists) vl_count_walkers(v, walks && !(pf & PF_DUP), lane);
+  if (!slots) vl_count_walkers(v, walks && !(pf & PF_DUP), lane);
   if (act && lane == 0) {
     const float2 d = make_float2(rho, rhoNear);
     v.density[i] = d;
     v.sdens[myslot] = d;
-    v.edens[r] = d;
-    uint32_t npf = pf;
-    bool use = listed;
-    if (rebuild) {
-      const uint32_t cnt = lcount;
-      v.ncount[r] = cnt;
-      v.xlist[r] = pi;
-      v.epos[r] = pi;
-      npf = (cnt > NLT) ? (npf & ~PF_LOK) : (npf | PF_LOK);
-      // the fresh list holds exactly this substep's pairs when complete and
-      // no two of the 27 buckets coincide: the displacement pass reads it
-      use = cnt <= NLT && !(pf & PF_DUP);
+    if (!slots) {
+      v.edens[r] = d;
+      v.erec[r].w = listed ? (pf | PF_LIST) : (pf & ~PF_LIST);
     }
-    npf = use ? (npf | PF_LIST) : (npf & ~PF_LIST);
-    v.pfl[i] = npf;
   }
 }
 
@@ -378,11 +424,17 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
   const int lane = threadIdx.x & (GLF - 1);
   const uint32_t r = t / GLF;
   const bool slots = !P->use_lists;
-  uint32_t i, myslot;
+  uint32_t i, myslot, pf = 0;
   bool act;
-  vl_group(v, r, slots, i, myslot, act);
+  if (slots) {
+    vl_group(v, r, true, i, myslot, act);
+  } else {
+    const uint4 rc = (r < (uint32_t)v.N) ? v.erec[r] : make_uint4(NO_RANK, 0u, 0u, 0u);
+    i = rc.x; myslot = rc.y; pf = rc.w;
+    act = i != NO_RANK && i >= (uint32_t)v.S && r < (uint32_t)v.N && v.ep[r] == i;
+  }
   if (!__any_sync(FULL, act)) return;
-  const bool listed = act && (v.pfl[i] & PF_LIST);
+  const bool listed = act && (pf & PF_LIST);
   const bool walks = act && !listed;
   const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
   const float4 pi = act ? (slots ? v.spos[myslot] : v.epos[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -425,13 +477,24 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
     const uint32_t* __restrict__ lst = v.nbr + r;
     const float4* __restrict__ epos = v.epos;
     const float2* __restrict__ edens = v.edens;
-    for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[(size_t)c * NS]);
-      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * NS]) : j0;
-      const float4 p0 = epos[j0], p1 = epos[j1];
-      const float2 d0 = edens[j0], d1 = edens[j1];
-      pair(p0, d0);
-      if (c + GLF < n) pair(p1, d1);
+    for (uint32_t c = (uint32_t)lane; c < n; c += 4 * GLF) {  // four entries' loads in flight
+      uint32_t j[4];
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        const uint32_t cw = c + (uint32_t)(w * GLF);
+        j[w] = (cw < n) ? __ldg(&lst[(size_t)cw * NS]) : NO_RANK;
+      }
+      float4 pj[4];
+      float2 dj[4];
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        const uint32_t jj = (j[w] != NO_RANK) ? j[w] : j[0];
+        pj[w] = epos[jj];
+        dj[w] = edens[jj];
+      }
+#pragma unroll
+      for (int w = 0; w < 4; w++)
+        if (j[w] != NO_RANK) pair(pj[w], dj[w]);
     }
   }
 #pragma unroll
@@ -480,21 +543,28 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
   const int lane = threadIdx.x & (GLF - 1);
   const uint32_t r = t / GLF;
   const bool slots = !P->use_lists;
-  uint32_t i, myslot;
-  bool fluid;
-  vl_group(v, r, slots, i, myslot, fluid);
-  const bool act = fluid && (v.flags[i] & F_ACTIVE);
+  uint32_t i, myslot, h = 0, pf = 0;
+  bool act;
+  if (slots) {
+    bool fluid;
+    vl_group(v, r, true, i, myslot, fluid);
+    act = fluid && (v.flags[i] & F_ACTIVE);
+  } else {
+    const uint4 rc = (r < (uint32_t)v.N) ? v.erec[r] : make_uint4(NO_RANK, 0u, 0u, 0u);
+    i = rc.x; myslot = rc.y; h = rc.z; pf = rc.w;
+    // culled by this substep's bounds pass: no xsph of its own
+    act = i != NO_RANK && i >= (uint32_t)v.S && r < (uint32_t)v.N && v.ep[r] == i && !(pf & PF_CULLED);
+  }
   if (!__any_sync(FULL, act)) return;
   // the bounds pass wrote the final position to both copies
   const float4 pi = act ? (slots ? v.spos[myslot] : v.epos[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
   const float H = P->fluid_h, H2 = H * H;
   const float allow = vl_allowance(P), rec = VMOVE_REC * allow;
-  const uint32_t pf = act ? v.pfl[i] : 0u;
   const float mv = (act && !slots) ? v.smove[r] : 0.f;
   const bool cand = act && !slots && (pf & (PF_LOK | PF_DUPF)) == PF_LOK && mv + rec <= allow;
   // a particle that kept its cell reads its grid bucket's fast mark; one that
   // changed cell takes the per-bucket test
-  const bool quick = cand && !(pf & PF_MOVED) && v.bfast[v.cell[i]] == 0u &&
+  const bool quick = cand && !(pf & PF_MOVED) && v.bfast[h] == 0u &&
                      mv + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
   const bool need = cand && !quick;
   bool listed = quick;
@@ -526,23 +596,30 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
     const uint32_t* __restrict__ lst = v.nbr + r;
     const float4* __restrict__ epos = v.epos;
     const float4* __restrict__ evel = v.evel;
-    for (uint32_t c = (uint32_t)lane; c < n; c += 2 * GLF) {  // two entries' loads in flight
-      const uint32_t j0 = __ldg(&lst[(size_t)c * NS]);
-      const uint32_t j1 = (c + GLF < n) ? __ldg(&lst[(size_t)(c + GLF) * NS]) : j0;
-      const float4 p0 = epos[j0], p1 = epos[j1];
-      const float4 u0 = evel[j0], u1 = evel[j1];
-      float ex = p0.x - pi.x, ey = p0.y - pi.y, ez = p0.z - pi.z;
-      bool in = dot3(ex, ey, ez, ex, ey, ez) < H2;
-      // a neighbour that changed cell after the grid build counts when its
-      // grid bucket is one of this particle's 27
-      if (in && u0.w != 0.f) in = vl_member(v, P, pi, v.ep[j0]);
-      sx = sx + (in ? u0.x : 0.f); sy = sy + (in ? u0.y : 0.f); sz = sz + (in ? u0.z : 0.f);
-      m = m + (in ? 1.0f : 0.f);
-      ex = p1.x - pi.x; ey = p1.y - pi.y; ez = p1.z - pi.z;
-      in = (c + GLF < n) && dot3(ex, ey, ez, ex, ey, ez) < H2;
-      if (in && u1.w != 0.f) in = vl_member(v, P, pi, v.ep[j1]);
-      sx = sx + (in ? u1.x : 0.f); sy = sy + (in ? u1.y : 0.f); sz = sz + (in ? u1.z : 0.f);
-      m = m + (in ? 1.0f : 0.f);
+    for (uint32_t c = (uint32_t)lane; c < n; c += 4 * GLF) {  // four entries' loads in flight
+      uint32_t j[4];
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        const uint32_t cw = c + (uint32_t)(w * GLF);
+        j[w] = (cw < n) ? __ldg(&lst[(size_t)cw * NS]) : NO_RANK;
+      }
+      float4 pj[4], uj[4];
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        const uint32_t jj = (j[w] != NO_RANK) ? j[w] : j[0];
+        pj[w] = epos[jj];
+        uj[w] = evel[jj];
+      }
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        const float ex = pj[w].x - pi.x, ey = pj[w].y - pi.y, ez = pj[w].z - pi.z;
+        bool in = j[w] != NO_RANK && dot3(ex, ey, ez, ex, ey, ez) < H2;
+        // a neighbour that changed cell after the grid build counts when its
+        // grid bucket is one of this particle's 27
+        if (in && uj[w].w != 0.f) in = vl_member(v, P, pi, v.ep[j[w]]);
+        sx = sx + (in ? uj[w].x : 0.f); sy = sy + (in ? uj[w].y : 0.f); sz = sz + (in ? uj[w].z : 0.f);
+        m = m + (in ? 1.0f : 0.f);
+      }
     }
   }
   sx = lane_sum<GLF>(sx);
@@ -551,7 +628,7 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
   m = lane_sum<GLF>(m);
   if (!slots) vl_count_walkers(v, walks && !(pf & PF_DUPF), lane);
   if (act && lane == 0) {
-    const float4 vi = v.vel[i];
+    const float4 vi = slots ? v.vel[i] : v.evel[r];  // the velocity pass's result either way
     float vx = vi.x, vy = vi.y, vz = vi.z;
     if (m > 0.f) {
       const float mu = P->viscosity;
