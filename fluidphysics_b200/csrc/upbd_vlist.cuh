@@ -205,95 +205,111 @@ __device__ __forceinline__ void vl_density_list(const SimView& v, uint32_t r, in
   }
 }
 
-// fluidDensity (src/gpu/wgsl.js:254-279) at a rebuild substep: sets the rank
-// order to this substep's grid order and writes the lists (the list kernel
-// below has nothing to do then). Returns at once on other substeps.
+// Walk of the groups that cannot read their lists: where one or two groups
+// of a warp walk, all 32 lanes load their candidates for them in turn
+// (lane_staged); where more do, each walks its own share. Every lane of the
+// warp calls it.
+template <class Load, class Use>
+__device__ __forceinline__ void vl_walk(const SimView& v, const CellHash& ch, int lane, bool walks, Load&& load,
+                                        Use&& use) {
+  const unsigned wg = __ballot_sync(0xffffffffu, walks && lane == 0);
+  if (wg == 0u) return;
+  if (__popc(wg) <= 2)
+    lane_staged<0, GLF>(v, ch, lane, walks, load, use);
+  else
+    lane_strided<0, GLF>(v, ch, lane, walks, load, use);
+}
+
+// fluidDensity (src/gpu/wgsl.js:254-279) at a rebuild substep, one warp per
+// particle: sets the rank order to this substep's grid order and writes the
+// lists (the list kernel below has nothing to do then). Returns at once on
+// other substeps.
+//
+// The reference's density over the 27 cells (every bucket visit counted,
+// coinciding buckets included) and, for the list, every fluid candidate
+// within R met at the visit of its own cell (so a bucket met through two
+// cells lists it once); then the cells past the 27 that R reaches. The lanes
+// place their entries by a ballot, so a list holds its candidates in walk
+// order (deterministic sums). At a rebuild a candidate's rank is its slot.
 __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const DevParams* __restrict__ P,
                                                      uint32_t vb) {
   const unsigned FULL = 0xffffffffu;
   if (v.scratch[SCR_REBUILD] == 0u) return;  // one value for the whole scene
   if (vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
   const uint32_t t = UPBD_VTID;
-  const int lane = threadIdx.x & (GLF - 1);
-  const uint32_t r = t / GLF;  // this group's rank = its slot
+  const int lane = threadIdx.x & 31;
+  const uint32_t r = t >> 5;  // this warp's rank = its slot
   uint32_t i, myslot;
   bool act;
-  vl_group(v, r, true, i, myslot, act);
+  vl_group(v, r, true, i, myslot, act);  // the same for every lane of the warp
   if (lane == 0 && r < (uint32_t)v.N) {  // the new rank order
     v.ep[r] = i;
     if (i != NO_RANK) v.erank[i] = r;
   }
-  if (!__any_sync(FULL, act)) return;
-  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (!act) return;  // the whole warp
+  const float4 pi = v.spos[myslot];
   const uint32_t NS = (uint32_t)v.N;
-  const uint32_t pf = act ? v.pfl[i] : 0u;
   const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
-  CellHash ch;
-  group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  float rho = 0.f, rhoNear = 0.f;
-  const float4* __restrict__ spos = v.spos;
-  uint32_t lcount = 0;
-  // The reference's density over the 27 cells (every bucket visit counted,
-  // coinciding buckets included) and, for the list, every fluid candidate
-  // within R met at the visit of its own cell (so a bucket met through two
-  // cells lists it once); then the cells past the 27 that R reaches. The
-  // group's lanes step together and place their entries by a ballot, so the
-  // list holds the candidates in walk order (deterministic sums). At a
-  // rebuild a candidate's rank is its slot.
+  const float R = H * (1.0f + VSKIN), R2 = R * R;
   const double inv = P->inv_cell;
   const double cx = floor(__dmul_rn((double)pi.x, inv)), cy = floor(__dmul_rn((double)pi.y, inv)),
                cz = floor(__dmul_rn((double)pi.z, inv));
-  const float R = H * (1.0f + VSKIN), R2 = R * R;
+  CellHash ch;
+  group_cell_hash<32>(pi.x, pi.y, pi.z, inv, ch);
+  const float4* __restrict__ spos = v.spos;
   uint32_t* __restrict__ lst = v.nbr + r;
-  const unsigned gmask = 0xFu << ((threadIdx.x & 31) & ~(unsigned)(GLF - 1));
-  const unsigned lt = gmask & ((1u << (threadIdx.x & 31)) - 1u);  // group lanes below this one
+  const unsigned lt = (1u << lane) - 1u;
+  uint32_t lcount = 0;
   auto place = [&](bool kp, uint32_t e) {
-    const unsigned bal = __ballot_sync(gmask, kp);
+    const unsigned bal = __ballot_sync(FULL, kp);
     if (kp) {
       const uint32_t c = lcount + (uint32_t)__popc(bal & lt);
       if (c < NLT) lst[(size_t)c * NS] = e;
     }
     lcount += (uint32_t)__popc(bal);
   };
-  const int g = (int)threadIdx.x / GLF;
-  const uint32_t run = walk_tables<0, GLF>(v, ch, lane, act, g);
-  uint32_t k = 0, next = s_walk_off[g][1], base = s_walk_base[g][0];
-  for (uint32_t c0 = 0; c0 < run; c0 += GLF) {  // the same trip count for the group's lanes
-    const uint32_t c = c0 + (uint32_t)lane;
-    bool kp = false;
-    uint32_t e = 0;
-    if (c < run) {
-      while (c >= next) {
-        k++;
-        next = s_walk_off[g][k + 1];
-        base = s_walk_base[g][k];
+  float rho = 0.f, rhoNear = 0.f;
+  const int g = (int)(threadIdx.x >> 5) * (32 / GLF);  // this warp's first walk-table row
+  {  // the 27 cells
+    const uint32_t run = walk_tables<0, 32>(v, ch, lane, true, g);
+    uint32_t k = 0, next = s_walk_off[g][1], base = s_walk_base[g][0];
+    for (uint32_t c0 = 0; c0 < run; c0 += 32) {
+      const uint32_t c = c0 + (uint32_t)lane;
+      bool kp = false;
+      uint32_t e = 0;
+      if (c < run) {
+        while (c >= next) {
+          k++;
+          next = s_walk_off[g][k + 1];
+          base = s_walk_base[g][k];
+        }
+        e = base + c;
+        const float4 pj = spos[e];
+        const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+        const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+        const bool in = (e != myslot) && (d2 < H2);
+        const float q = 1.0f - approx_sqrt(d2) * invH;
+        const float qq = in ? q * q : 0.0f;
+        rho = rho + qq;
+        rhoNear = rhoNear + qq * q;
+        if (e != myslot && d2 < R2) {
+          const int a = (int)k / 9 - 1, b = ((int)k / 3) % 3 - 1, cc = (int)k % 3 - 1;
+          kp = vl_in_cell(pj, inv, cx + a, cy + b, cz + cc);
+        }
       }
-      e = base + c;
-      const float4 pj = spos[e];
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      const bool in = (e != myslot) && (d2 < H2);
-      const float q = 1.0f - approx_sqrt(d2) * invH;
-      const float qq = in ? q * q : 0.0f;
-      rho = rho + qq;
-      rhoNear = rhoNear + qq * q;
-      if (e != myslot && d2 < R2) {
-        const int a = (int)k / 9 - 1, b = ((int)k / 3) % 3 - 1, cc = (int)k % 3 - 1;
-        kp = vl_in_cell(pj, inv, cx + a, cy + b, cz + cc);
-      }
+      place(kp, e);
     }
-    place(kp, e);
+    __syncwarp();
   }
-  __syncwarp();  // the walk tables are free again
-  if (act) {
-    // reach of R past the 27 cells, in cells (R is below two cells)
+  {  // the cells past the 27 that R reaches (R is below two cells)
     const double ext = (double)R * inv - 1.0 + 1e-3, rc2 = ((double)R * inv) * ((double)R * inv) * 1.0001;
     const double fx = __dmul_rn((double)pi.x, inv) - cx, fy = __dmul_rn((double)pi.y, inv) - cy,
                  fz = __dmul_rn((double)pi.z, inv) - cz;
     const int lox = (fx < ext) ? -2 : -1, hix = (1.0 - fx < ext) ? 2 : 1;
     const int loy = (fy < ext) ? -2 : -1, hiy = (1.0 - fy < ext) ? 2 : 1;
     const int loz = (fz < ext) ? -2 : -1, hiz = (1.0 - fz < ext) ? 2 : 1;
-    if (lox < -1 || hix > 1 || loy < -1 || hiy > 1 || loz < -1 || hiz > 1) {
+    const int nx = hix - lox + 1, ny = hiy - loy + 1, nz = hiz - loz + 1, nbox = nx * ny * nz;  // <= 64
+    if (nbox > 27) {
       const int32_t xm2 = js_toint32(__dmul_rn(__dadd_rn(cx, -2.0), 92837111.0));
       const int32_t xp2 = js_toint32(__dmul_rn(__dadd_rn(cx, 2.0), 92837111.0));
       const int32_t ym2 = js_toint32(__dmul_rn(__dadd_rn(cy, -2.0), 689287499.0));
@@ -301,36 +317,72 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
       const int32_t zm2 = js_toint32(__dmul_rn(__dadd_rn(cz, -2.0), 283923481.0));
       const int32_t zp2 = js_toint32(__dmul_rn(__dadd_rn(cz, 2.0), 283923481.0));
       const uint32_t mask = (uint32_t)v.T - 1u;
-      for (int a = lox; a <= hix; a++)
-        for (int b = loy; b <= hiy; b++)
-          for (int c = loz; c <= hiz; c++) {
-            if (a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1) continue;  // one of the 27
-            // distance (in cells) from the particle to the cell's box
-            const double gx = (a < 0) ? fx + (double)(-a - 1) : ((a > 0) ? (1.0 - fx) + (double)(a - 1) : 0.0);
-            const double gy = (b < 0) ? fy + (double)(-b - 1) : ((b > 0) ? (1.0 - fy) + (double)(b - 1) : 0.0);
-            const double gz = (c < 0) ? fz + (double)(-c - 1) : ((c > 0) ? (1.0 - fz) + (double)(c - 1) : 0.0);
-            if (gx * gx + gy * gy + gz * gz > rc2) continue;
+      // box cell k (two per lane) -> its fluid range when it is past the 27
+      // and within R; the ranges become one sequence (offsets by a warp scan)
+      // in the warp's spare walk-table rows, read as flat arrays
+      uint32_t* xb = &s_walk_base[g + 1][0];  // 7 rows x 28 >= 64 entries
+      uint32_t* xo = &s_walk_off[g + 1][0];
+      uint32_t run = 0;
+#pragma unroll
+      for (int half = 0; half < 2; half++) {
+        const int k = lane + 32 * half;
+        uint32_t s0 = 0, n = 0;
+        if (k < nbox) {
+          const int a = lox + k / (ny * nz), b = loy + (k / nz) % ny, c = loz + k % nz;
+          const bool core = a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1;
+          const double gx = (a < 0) ? fx + (double)(-a - 1) : ((a > 0) ? (1.0 - fx) + (double)(a - 1) : 0.0);
+          const double gy = (b < 0) ? fy + (double)(-b - 1) : ((b > 0) ? (1.0 - fy) + (double)(b - 1) : 0.0);
+          const double gz = (c < 0) ? fz + (double)(-c - 1) : ((c > 0) ? (1.0 - fz) + (double)(c - 1) : 0.0);
+          if (!core && gx * gx + gy * gy + gz * gz <= rc2) {
             const uint32_t h = (uint32_t)(vl_sel(a, xm2, ch.hx[0], ch.hx[1], ch.hx[2], xp2) ^
                                           vl_sel(b, ym2, ch.hy[0], ch.hy[1], ch.hy[2], yp2) ^
                                           vl_sel(c, zm2, ch.hz[0], ch.hz[1], ch.hz[2], zp2)) & mask;
-            const uint32_t s0 = __ldg(&v.start[h]), s1 = __ldg(&v.fend[h]);
-            for (uint32_t e0 = s0; e0 < s1; e0 += GLF) {  // the same trip count for the group's lanes
-              const uint32_t e = e0 + (uint32_t)lane;
-              bool kp = false;
-              if (e < s1) {
-                const float4 pj = spos[e];
-                const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-                kp = dot3(ex, ey, ez, ex, ey, ez) < R2 &&
-                     vl_in_cell(pj, inv, cx + (double)a, cy + (double)b, cz + (double)c);
-              }
-              place(kp, e);
-            }
+            s0 = __ldg(&v.start[h]);
+            n = __ldg(&v.fend[h]) - s0;
           }
+        }
+        uint32_t x = n;  // inclusive scan over the warp
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t y = __shfl_up_sync(FULL, x, d);
+          if (lane >= d) x += y;
+        }
+        const uint32_t off = run + x - n;
+        run += __shfl_sync(FULL, x, 31);
+        if (k < 64) {
+          xb[k] = s0 - off;
+          xo[k] = off;
+        }
+      }
+      if (lane == 0) xo[64] = run;
+      __syncwarp();
+      uint32_t k = 0, next = xo[1], base = xb[0];
+      for (uint32_t c0 = 0; c0 < run; c0 += 32) {
+        const uint32_t c = c0 + (uint32_t)lane;
+        bool kp = false;
+        uint32_t e = 0;
+        if (c < run) {
+          while (c >= next) {
+            k++;
+            next = xo[k + 1];
+            base = xb[k];
+          }
+          e = base + c;
+          const float4 pj = spos[e];
+          const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+          const int a = lox + (int)k / (ny * nz), b = loy + ((int)k / nz) % ny, cc = loz + (int)k % nz;
+          kp = dot3(ex, ey, ez, ex, ey, ez) < R2 &&
+               vl_in_cell(pj, inv, cx + (double)a, cy + (double)b, cz + (double)cc);
+        }
+        place(kp, e);
+      }
+      __syncwarp();
     }
   }
-  rho = lane_sum<GLF>(rho);
-  rhoNear = lane_sum<GLF>(rhoNear);
-  if (act && lane == 0) {
+  rho = lane_sum<32>(rho);
+  rhoNear = lane_sum<32>(rhoNear);
+  if (lane == 0) {
+    const uint32_t pf = v.pfl[i];
     const float2 d = make_float2(rho, rhoNear);
     v.density[i] = d;
     v.sdens[myslot] = d;
@@ -385,9 +437,9 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
   }
   const bool walks = act && !listed;
   float rho = 0.f, rhoNear = 0.f;
-  if (__any_sync(FULL, walks)) {
+  {
     const float4* __restrict__ spos = v.spos;
-    lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
+    vl_walk(v, ch, lane, walks, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
       const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
       const float d2 = dot3(ex, ey, ez, ex, ey, ez);
       const bool in = (e != myslot) && (d2 < H2);
@@ -466,10 +518,9 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
     };
     const float4* __restrict__ spos = v.spos;
     const float2* __restrict__ sdens = v.sdens;
-    lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return PD{spos[e], sdens[e]}; },
-                         [&](uint32_t e, const PD& c) {
-                           if (e != myslot) pair(c.p, c.d);
-                         });
+    vl_walk(v, ch, lane, walks, [&](uint32_t e) { return PD{spos[e], sdens[e]}; }, [&](uint32_t e, const PD& c) {
+      if (e != myslot) pair(c.p, c.d);
+    });
   }
   if (listed) {  // lane l reads entries l, l + GLF, ...
     const uint32_t NS = (uint32_t)v.N;
@@ -582,7 +633,7 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
     };
     const float4* __restrict__ spos = v.spos;
     const float4* __restrict__ svel = v.svel;
-    lane_strided<0, GLF>(v, ch, lane, walks, [&](uint32_t e) { return PV{spos[e], svel[e]}; },
+    vl_walk(v, ch, lane, walks, [&](uint32_t e) { return PV{spos[e], svel[e]}; },
                          [&](uint32_t e, const PV& c) {
                            const float ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
                            const bool in = (e != myslot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
