@@ -229,7 +229,7 @@ int launch_substep(upbd_sim* s, int last) {
 #ifndef UPBD_PARITY_BUILD
   // a rebuild substep's density (lists, rank order) in a launch of its own,
   // so the list launch keeps few registers; each returns on the other's substeps
-  PROF(s, K_DENSITY, k_density_rebuild<<<blocks_for((long long)v.N * 32), 256, 0, st>>>(v, P));  // a warp per slot
+  PROF(s, K_DENSITY, k_density_rebuild<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
 #endif
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));

@@ -47,7 +47,6 @@ enum Domain {
   D_SGL,      // GL lanes per solid (apply + contact marks)
   D_S,        // solids
   D_BC,       // bond/tet updates rounded to warps + GL lanes per particle
-  D_W,        // a warp per grid slot (the product build's density rebuild)
   NUM_DOMAINS
 };
 
@@ -128,7 +127,7 @@ __global__ void __launch_bounds__(256, 6) kb_density(BatchArgs a) {
 }
 #ifndef UPBD_PARITY_BUILD
 __global__ void __launch_bounds__(256) kb_density_rebuild(BatchArgs a) {
-  batch_loop<D_W, false, true>(a, UPBD_BODY { b_density_rebuild_vl(v, P, vb); });
+  batch_loop<D_FGL, false, true>(a, UPBD_BODY { b_density_rebuild_vl(v, P, vb); });
 }
 #endif
 template <bool APPLY>
@@ -219,7 +218,6 @@ void scene_blocks(const SimView& v, bool tets, int bt, uint32_t out[NUM_DOMAINS]
   out[D_SGL] = ceil_div((long long)v.S * GL, bt);
   out[D_S] = ceil_div(v.S, bt);
   out[D_BC] = ceil_div((long long)bond_pad_of(v.C, nt) + (long long)v.N * GL, bt);
-  out[D_W] = ceil_div((long long)v.N * 32, bt);
 }
 
 // First-fit allocator over device chunks (256-byte granules), coalescing on

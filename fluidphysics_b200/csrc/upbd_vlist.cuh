@@ -220,25 +220,21 @@ __device__ __forceinline__ void vl_walk(const SimView& v, const CellHash& ch, in
     lane_strided<0, GLF>(v, ch, lane, walks, load, use);
 }
 
-// fluidDensity (src/gpu/wgsl.js:254-279) at a rebuild substep, one warp per
-// particle: sets the rank order to this substep's grid order and writes the
-// lists (the list kernel below has nothing to do then). Returns at once on
-// other substeps.
+// fluidDensity (src/gpu/wgsl.js:254-279) at a rebuild for the particle of
+// rank r (its slot in this substep's grid), with the whole warp: its density
+// and its list.
 //
 // The reference's density over the 27 cells (every bucket visit counted,
 // coinciding buckets included) and, for the list, every fluid candidate
-// within R met at the visit of its own cell (so a bucket met through two
-// cells lists it once); then the cells past the 27 that R reaches. The lanes
-// place their entries by a ballot, so a list holds its candidates in walk
-// order (deterministic sums). At a rebuild a candidate's rank is its slot.
-__device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const DevParams* __restrict__ P,
-                                                     uint32_t vb) {
+// within R of the cells that R reaches: the 27 and those past them. When two
+// of the visited cells share a bucket, a candidate is taken only at the
+// visit of its own cell (so it is listed once); otherwise every candidate
+// within R lies in the cell it was met through. The lanes place their entries
+// by a ballot, so a list holds its candidates in walk order (deterministic
+// sums). At a rebuild a candidate's rank is its slot.
+__device__ __forceinline__ void vl_rebuild_one(const SimView& v, const DevParams* __restrict__ P, uint32_t r,
+                                               int lane, int g) {
   const unsigned FULL = 0xffffffffu;
-  if (v.scratch[SCR_REBUILD] == 0u) return;  // one value for the whole scene
-  if (vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
-  const uint32_t t = UPBD_VTID;
-  const int lane = threadIdx.x & 31;
-  const uint32_t r = t >> 5;  // this warp's rank = its slot
   uint32_t i, myslot;
   bool act;
   vl_group(v, r, true, i, myslot, act);  // the same for every lane of the warp
@@ -256,6 +252,62 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
                cz = floor(__dmul_rn((double)pi.z, inv));
   CellHash ch;
   group_cell_hash<32>(pi.x, pi.y, pi.z, inv, ch);
+  const uint32_t mask = (uint32_t)v.T - 1u;
+  // the box of cells that R reaches (R is below two cells)
+  const double ext = (double)R * inv - 1.0 + 1e-3, rc2 = ((double)R * inv) * ((double)R * inv) * 1.0001;
+  const double fx = __dmul_rn((double)pi.x, inv) - cx, fy = __dmul_rn((double)pi.y, inv) - cy,
+               fz = __dmul_rn((double)pi.z, inv) - cz;
+  const int lox = (fx < ext) ? -2 : -1, hix = (1.0 - fx < ext) ? 2 : 1;
+  const int loy = (fy < ext) ? -2 : -1, hiy = (1.0 - fy < ext) ? 2 : 1;
+  const int loz = (fz < ext) ? -2 : -1, hiz = (1.0 - fz < ext) ? 2 : 1;
+  const int ny = hiy - loy + 1, nz = hiz - loz + 1, nbox = (hix - lox + 1) * ny * nz;  // <= 64
+  const int32_t xm2 = js_toint32(__dmul_rn(__dadd_rn(cx, -2.0), 92837111.0));
+  const int32_t xp2 = js_toint32(__dmul_rn(__dadd_rn(cx, 2.0), 92837111.0));
+  const int32_t ym2 = js_toint32(__dmul_rn(__dadd_rn(cy, -2.0), 689287499.0));
+  const int32_t yp2 = js_toint32(__dmul_rn(__dadd_rn(cy, 2.0), 689287499.0));
+  const int32_t zm2 = js_toint32(__dmul_rn(__dadd_rn(cz, -2.0), 283923481.0));
+  const int32_t zp2 = js_toint32(__dmul_rn(__dadd_rn(cz, 2.0), 283923481.0));
+  // box cells k = lane and lane + 32: visited (one of the 27, or past them and
+  // within R) -> bucket and fluid range; bv = NO_RANK for cells not visited
+  uint32_t bv[2], s0[2], n[2];
+  bool extra[2];
+#pragma unroll
+  for (int half = 0; half < 2; half++) {
+    const int k = lane + 32 * half;
+    bv[half] = NO_RANK;
+    s0[half] = 0u;
+    n[half] = 0u;
+    extra[half] = false;
+    if (k < nbox) {
+      const int a = lox + k / (ny * nz), b = loy + (k / nz) % ny, c = loz + k % nz;
+      const bool core = a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1;
+      const double gx = (a < 0) ? fx + (double)(-a - 1) : ((a > 0) ? (1.0 - fx) + (double)(a - 1) : 0.0);
+      const double gy = (b < 0) ? fy + (double)(-b - 1) : ((b > 0) ? (1.0 - fy) + (double)(b - 1) : 0.0);
+      const double gz = (c < 0) ? fz + (double)(-c - 1) : ((c > 0) ? (1.0 - fz) + (double)(c - 1) : 0.0);
+      if (core || gx * gx + gy * gy + gz * gz <= rc2) {
+        bv[half] = (uint32_t)(vl_sel(a, xm2, ch.hx[0], ch.hx[1], ch.hx[2], xp2) ^
+                              vl_sel(b, ym2, ch.hy[0], ch.hy[1], ch.hy[2], yp2) ^
+                              vl_sel(c, zm2, ch.hz[0], ch.hz[1], ch.hz[2], zp2)) & mask;
+        if (!core) {
+          extra[half] = true;
+          s0[half] = __ldg(&v.start[bv[half]]);
+          n[half] = __ldg(&v.fend[bv[half]]) - s0[half];
+        }
+      }
+    }
+  }
+  // do two visited cells share a bucket?
+  bool dup = false;
+#pragma unroll
+  for (int half = 0; half < 2; half++) {
+    const unsigned same = __match_any_sync(FULL, bv[half]);
+    dup = dup || (bv[half] != NO_RANK && __popc(same) > 1);
+  }
+  for (int d = 0; d < 32; d++) {
+    const uint32_t o = __shfl_sync(FULL, bv[1], d);
+    dup = dup || (bv[0] != NO_RANK && bv[0] == o);
+  }
+  const bool check = __any_sync(FULL, dup);
   const float4* __restrict__ spos = v.spos;
   uint32_t* __restrict__ lst = v.nbr + r;
   const unsigned lt = (1u << lane) - 1u;
@@ -269,7 +321,6 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
     lcount += (uint32_t)__popc(bal);
   };
   float rho = 0.f, rhoNear = 0.f;
-  const int g = (int)(threadIdx.x >> 5) * (32 / GLF);  // this warp's first walk-table row
   {  // the 27 cells
     const uint32_t run = walk_tables<0, 32>(v, ch, lane, true, g);
     uint32_t k = 0, next = s_walk_off[g][1], base = s_walk_base[g][0];
@@ -292,7 +343,8 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
         const float qq = in ? q * q : 0.0f;
         rho = rho + qq;
         rhoNear = rhoNear + qq * q;
-        if (e != myslot && d2 < R2) {
+        kp = e != myslot && d2 < R2;
+        if (kp && check) {
           const int a = (int)k / 9 - 1, b = ((int)k / 3) % 3 - 1, cc = (int)k % 3 - 1;
           kp = vl_in_cell(pj, inv, cx + a, cy + b, cz + cc);
         }
@@ -301,83 +353,51 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
     }
     __syncwarp();
   }
-  {  // the cells past the 27 that R reaches (R is below two cells)
-    const double ext = (double)R * inv - 1.0 + 1e-3, rc2 = ((double)R * inv) * ((double)R * inv) * 1.0001;
-    const double fx = __dmul_rn((double)pi.x, inv) - cx, fy = __dmul_rn((double)pi.y, inv) - cy,
-                 fz = __dmul_rn((double)pi.z, inv) - cz;
-    const int lox = (fx < ext) ? -2 : -1, hix = (1.0 - fx < ext) ? 2 : 1;
-    const int loy = (fy < ext) ? -2 : -1, hiy = (1.0 - fy < ext) ? 2 : 1;
-    const int loz = (fz < ext) ? -2 : -1, hiz = (1.0 - fz < ext) ? 2 : 1;
-    const int nx = hix - lox + 1, ny = hiy - loy + 1, nz = hiz - loz + 1, nbox = nx * ny * nz;  // <= 64
-    if (nbox > 27) {
-      const int32_t xm2 = js_toint32(__dmul_rn(__dadd_rn(cx, -2.0), 92837111.0));
-      const int32_t xp2 = js_toint32(__dmul_rn(__dadd_rn(cx, 2.0), 92837111.0));
-      const int32_t ym2 = js_toint32(__dmul_rn(__dadd_rn(cy, -2.0), 689287499.0));
-      const int32_t yp2 = js_toint32(__dmul_rn(__dadd_rn(cy, 2.0), 689287499.0));
-      const int32_t zm2 = js_toint32(__dmul_rn(__dadd_rn(cz, -2.0), 283923481.0));
-      const int32_t zp2 = js_toint32(__dmul_rn(__dadd_rn(cz, 2.0), 283923481.0));
-      const uint32_t mask = (uint32_t)v.T - 1u;
-      // box cell k (two per lane) -> its fluid range when it is past the 27
-      // and within R; the ranges become one sequence (offsets by a warp scan)
-      // in the warp's spare walk-table rows, read as flat arrays
-      uint32_t* xb = &s_walk_base[g + 1][0];  // 7 rows x 28 >= 64 entries
-      uint32_t* xo = &s_walk_off[g + 1][0];
-      uint32_t run = 0;
+  if (__any_sync(FULL, extra[0] || extra[1])) {
+    // the cells past the 27 as one sequence (offsets by a warp scan) in the
+    // warp's spare walk-table rows, read as flat arrays
+    uint32_t* xb = &s_walk_base[g + 1][0];  // 7 rows x 28 >= 65 entries
+    uint32_t* xo = &s_walk_off[g + 1][0];
+    uint32_t run = 0;
 #pragma unroll
-      for (int half = 0; half < 2; half++) {
-        const int k = lane + 32 * half;
-        uint32_t s0 = 0, n = 0;
-        if (k < nbox) {
-          const int a = lox + k / (ny * nz), b = loy + (k / nz) % ny, c = loz + k % nz;
-          const bool core = a >= -1 && a <= 1 && b >= -1 && b <= 1 && c >= -1 && c <= 1;
-          const double gx = (a < 0) ? fx + (double)(-a - 1) : ((a > 0) ? (1.0 - fx) + (double)(a - 1) : 0.0);
-          const double gy = (b < 0) ? fy + (double)(-b - 1) : ((b > 0) ? (1.0 - fy) + (double)(b - 1) : 0.0);
-          const double gz = (c < 0) ? fz + (double)(-c - 1) : ((c > 0) ? (1.0 - fz) + (double)(c - 1) : 0.0);
-          if (!core && gx * gx + gy * gy + gz * gz <= rc2) {
-            const uint32_t h = (uint32_t)(vl_sel(a, xm2, ch.hx[0], ch.hx[1], ch.hx[2], xp2) ^
-                                          vl_sel(b, ym2, ch.hy[0], ch.hy[1], ch.hy[2], yp2) ^
-                                          vl_sel(c, zm2, ch.hz[0], ch.hz[1], ch.hz[2], zp2)) & mask;
-            s0 = __ldg(&v.start[h]);
-            n = __ldg(&v.fend[h]) - s0;
-          }
-        }
-        uint32_t x = n;  // inclusive scan over the warp
+    for (int half = 0; half < 2; half++) {
+      const int k = lane + 32 * half;
+      uint32_t x = n[half];  // inclusive scan over the warp
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const uint32_t y = __shfl_up_sync(FULL, x, d);
-          if (lane >= d) x += y;
-        }
-        const uint32_t off = run + x - n;
-        run += __shfl_sync(FULL, x, 31);
-        if (k < 64) {
-          xb[k] = s0 - off;
-          xo[k] = off;
-        }
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, d);
+        if (lane >= d) x += y;
       }
-      if (lane == 0) xo[64] = run;
-      __syncwarp();
-      uint32_t k = 0, next = xo[1], base = xb[0];
-      for (uint32_t c0 = 0; c0 < run; c0 += 32) {
-        const uint32_t c = c0 + (uint32_t)lane;
-        bool kp = false;
-        uint32_t e = 0;
-        if (c < run) {
-          while (c >= next) {
-            k++;
-            next = xo[k + 1];
-            base = xb[k];
-          }
-          e = base + c;
-          const float4 pj = spos[e];
-          const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-          const int a = lox + (int)k / (ny * nz), b = loy + ((int)k / nz) % ny, cc = loz + (int)k % nz;
-          kp = dot3(ex, ey, ez, ex, ey, ez) < R2 &&
-               vl_in_cell(pj, inv, cx + (double)a, cy + (double)b, cz + (double)cc);
-        }
-        place(kp, e);
-      }
-      __syncwarp();
+      const uint32_t off = run + x - n[half];
+      run += __shfl_sync(FULL, x, 31);
+      xb[k] = s0[half] - off;
+      xo[k] = off;
     }
+    if (lane == 0) xo[64] = run;
+    __syncwarp();
+    uint32_t k = 0, next = xo[1], base = xb[0];
+    for (uint32_t c0 = 0; c0 < run; c0 += 32) {
+      const uint32_t c = c0 + (uint32_t)lane;
+      bool kp = false;
+      uint32_t e = 0;
+      if (c < run) {
+        while (c >= next) {
+          k++;
+          next = xo[k + 1];
+          base = xb[k];
+        }
+        e = base + c;
+        const float4 pj = spos[e];
+        const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+        kp = dot3(ex, ey, ez, ex, ey, ez) < R2;
+        if (kp && check) {
+          const int a = lox + (int)k / (ny * nz), b = loy + ((int)k / nz) % ny, cc = loz + (int)k % nz;
+          kp = vl_in_cell(pj, inv, cx + (double)a, cy + (double)b, cz + (double)cc);
+        }
+      }
+      place(kp, e);
+    }
+    __syncwarp();
   }
   rho = lane_sum<32>(rho);
   rhoNear = lane_sum<32>(rhoNear);
@@ -398,6 +418,22 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
     const uint32_t rpf = (npf & (PF_DUP | PF_LOK)) | ((ok && !(pf & PF_DUP)) ? PF_LIST : 0u);
     v.erec[r] = make_uint4(i, myslot, v.cell[i], rpf);
   }
+  __syncwarp();  // the walk tables are reused by the next rank
+}
+
+// fluidDensity (src/gpu/wgsl.js:254-279) at a rebuild substep: sets the rank
+// order to this substep's grid order and writes the lists (the list kernel
+// below has nothing to do then); returns at once on other substeps. Tile vb
+// covers ranks vb * blockDim.x / GLF onwards, each warp 32 / GLF of them in
+// turn, each with all 32 lanes.
+__device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const DevParams* __restrict__ P,
+                                                     uint32_t vb) {
+  if (v.scratch[SCR_REBUILD] == 0u) return;  // one value for the whole scene
+  if (vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
+  const int lane = threadIdx.x & 31;
+  const int g = (int)(threadIdx.x >> 5) * (32 / GLF);  // this warp's first walk-table row
+  const uint32_t r0 = (UPBD_VTID >> 5) * (32 / GLF);
+  for (int k = 0; k < 32 / GLF; k++) vl_rebuild_one(v, P, r0 + (uint32_t)k, lane, g);
 }
 
 // fluidDensity (src/gpu/wgsl.js:254-279) on the substeps without a rebuild:
