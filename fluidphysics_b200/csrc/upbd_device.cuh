@@ -273,7 +273,7 @@ constexpr uint32_t NBR_IN = 0x80000000u;  // list entry flag: within H at densit
 // (the rest covers rounding): then every fluid particle within H is listed.
 // Movements at or below VMOVE_REC * the allowance are not recorded per
 // bucket: a bucket counts them as that much.
-constexpr float VSKIN = 0.25f;
+constexpr float VSKIN = 0.15f;
 constexpr float VMOVE_FRAC = 0.9f;
 constexpr float VMOVE_REC = 0.25f;
 // A particle that moved more than VFAST * the allowance since the rebuild

@@ -233,18 +233,18 @@ __device__ __forceinline__ void vl_walk(const SimView& v, const CellHash& ch, in
 // by a ballot, so a list holds its candidates in walk order (deterministic
 // sums). At a rebuild a candidate's rank is its slot.
 __device__ __forceinline__ void vl_rebuild_one(const SimView& v, const DevParams* __restrict__ P, uint32_t r,
-                                               int lane, int g) {
+                                               int lane, int g, uint32_t* __restrict__ lst, uint32_t& lcount) {
   const unsigned FULL = 0xffffffffu;
   uint32_t i, myslot;
   bool act;
   vl_group(v, r, true, i, myslot, act);  // the same for every lane of the warp
+  lcount = 0;
   if (lane == 0 && r < (uint32_t)v.N) {  // the new rank order
     v.ep[r] = i;
     if (i != NO_RANK) v.erank[i] = r;
   }
   if (!act) return;  // the whole warp
   const float4 pi = v.spos[myslot];
-  const uint32_t NS = (uint32_t)v.N;
   const float H = P->fluid_h, H2 = H * H, invH = 1.0f / H;
   const float R = H * (1.0f + VSKIN), R2 = R * R;
   const double inv = P->inv_cell;
@@ -309,14 +309,12 @@ __device__ __forceinline__ void vl_rebuild_one(const SimView& v, const DevParams
   }
   const bool check = __any_sync(FULL, dup);
   const float4* __restrict__ spos = v.spos;
-  uint32_t* __restrict__ lst = v.nbr + r;
   const unsigned lt = (1u << lane) - 1u;
-  uint32_t lcount = 0;
-  auto place = [&](bool kp, uint32_t e) {
+  auto place = [&](bool kp, uint32_t e) {  // into the warp's shared staging row
     const unsigned bal = __ballot_sync(FULL, kp);
     if (kp) {
       const uint32_t c = lcount + (uint32_t)__popc(bal & lt);
-      if (c < NLT) lst[(size_t)c * NS] = e;
+      if (c < NLT) lst[c] = e;
     }
     lcount += (uint32_t)__popc(bal);
   };
@@ -407,7 +405,7 @@ __device__ __forceinline__ void vl_rebuild_one(const SimView& v, const DevParams
     v.density[i] = d;
     v.sdens[myslot] = d;
     v.edens[r] = d;
-    v.ncount[r] = lcount;
+    v.ncount[r] = lcount;  // may exceed NLT: then the list is not used
     v.xlist[r] = pi;
     v.epos[r] = pi;
     const bool ok = lcount <= NLT;
@@ -430,10 +428,28 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
                                                      uint32_t vb) {
   if (v.scratch[SCR_REBUILD] == 0u) return;  // one value for the whole scene
   if (vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
-  const int lane = threadIdx.x & 31;
-  const int g = (int)(threadIdx.x >> 5) * (32 / GLF);  // this warp's first walk-table row
-  const uint32_t r0 = (UPBD_VTID >> 5) * (32 / GLF);
-  for (int k = 0; k < 32 / GLF; k++) vl_rebuild_one(v, P, r0 + (uint32_t)k, lane, g);
+  constexpr int RW = 32 / GLF;  // ranks per warp
+  __shared__ uint32_t s_lst[256 / 32][RW][NLT];  // each warp's lists before they are written out
+  const int lane = threadIdx.x & 31, w = (int)(threadIdx.x >> 5);
+  const int g = w * (32 / GLF);  // this warp's first walk-table row
+  const uint32_t r0 = (UPBD_VTID >> 5) * RW;
+  uint32_t cnt[RW];
+#pragma unroll
+  for (int k = 0; k < RW; k++) vl_rebuild_one(v, P, r0 + (uint32_t)k, lane, g, s_lst[w][k], cnt[k]);
+  __syncwarp();
+  // write out row by row: entry c of the warp's RW consecutive ranks is one
+  // run of RW words (lane: entry c0 + lane / RW of rank r0 + lane % RW)
+  uint32_t most = 0;
+#pragma unroll
+  for (int k = 0; k < RW; k++) most = max(most, min(cnt[k], NLT));
+  const int k = lane % RW;
+  const uint32_t NS = (uint32_t)v.N;
+  for (uint32_t c0 = 0; c0 < most; c0 += 32 / RW) {
+    const uint32_t c = c0 + (uint32_t)(lane / RW);
+    const uint32_t r = r0 + (uint32_t)k;
+    if (c < min(cnt[k], NLT) && r < NS) v.nbr[(size_t)c * NS + r] = s_lst[w][k][c];
+  }
+  __syncwarp();
 }
 
 // fluidDensity (src/gpu/wgsl.js:254-279) on the substeps without a rebuild:
