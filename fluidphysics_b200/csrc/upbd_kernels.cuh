@@ -69,13 +69,19 @@ __global__ void __launch_bounds__(256) k_rankfix(SimView v, const DevParams* __r
 #ifndef UPBD_PARITY_BUILD
 // Product build: a rebuild substep's density pass (returns at once on the
 // others, where k_density runs over the lists instead).
-__global__ void __launch_bounds__(256) k_density_rebuild(SimView v, const DevParams* __restrict__ P) {
+__global__ void __launch_bounds__(256, 4) k_density_rebuild(SimView v, const DevParams* __restrict__ P) {
   b_density_rebuild_vl(v, P, blockIdx.x);
 }
 #endif
 // The fluid gathers: the bucket walks in the parity build (the oracle's
-// summation order), lists kept across substeps in the product build.
-__global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __restrict__ P) {
+// summation order), lists kept across substeps in the product build (at 32
+// registers: eight blocks per SM, so a scene's groups are resident at once).
+#ifdef UPBD_PARITY_BUILD
+#define UPBD_GATHER_BOUNDS __launch_bounds__(256)
+#else
+#define UPBD_GATHER_BOUNDS __launch_bounds__(256, 8)
+#endif
+__global__ void UPBD_GATHER_BOUNDS k_density(SimView v, const DevParams* __restrict__ P) {
 #ifdef UPBD_PARITY_BUILD
   b_density(v, P, blockIdx.x);
 #else
@@ -83,7 +89,7 @@ __global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __r
 #endif
 }
 template <bool APPLY>
-__global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __restrict__ P) {
+__global__ void UPBD_GATHER_BOUNDS k_disp(SimView v, const DevParams* __restrict__ P) {
 #ifdef UPBD_PARITY_BUILD
   b_disp<APPLY>(v, P, blockIdx.x);
 #else
@@ -127,7 +133,7 @@ __global__ void __launch_bounds__(256) k_solid_visc(SimView v, const DevParams* 
 }
 __global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) { b_solid_visc_apply(v, blockIdx.x); }
 template <bool APPLY, int ROLE = 0>
-__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) {
+__global__ void UPBD_GATHER_BOUNDS k_xsph(SimView v, const DevParams* __restrict__ P) {
 #ifdef UPBD_PARITY_BUILD
   b_xsph<APPLY, ROLE>(v, P, blockIdx.x);
 #else

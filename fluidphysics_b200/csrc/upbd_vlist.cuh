@@ -43,6 +43,10 @@
 
 namespace upbd {
 
+// list entries whose loads are in flight together per lane (the list
+// kernels run at 32 registers so that all their blocks are resident at once)
+constexpr int VLF = 2;
+
 __device__ __forceinline__ float vl_allowance(const DevParams* __restrict__ P) {
   return VSKIN * P->fluid_h * VMOVE_FRAC;
 }
@@ -176,25 +180,25 @@ __device__ __forceinline__ void vl_group(const SimView& v, uint32_t r, bool slot
 }
 
 // Density of one group over its list (lane l: entries l, l + GLF, ...,
-// four entries' loads in flight).
+// VLF entries' loads in flight).
 __device__ __forceinline__ void vl_density_list(const SimView& v, uint32_t r, int lane, const float4& pi, float H2,
                                                 float invH, float& rho, float& rhoNear) {
   const uint32_t NS = (uint32_t)v.N;
   const uint32_t n = v.ncount[r];
   const uint32_t* __restrict__ lst = v.nbr + r;
   const float4* __restrict__ epos = v.epos;
-  for (uint32_t c = (uint32_t)lane; c < n; c += 4 * GLF) {
-    uint32_t j[4];
+  for (uint32_t c = (uint32_t)lane; c < n; c += VLF * GLF) {
+    uint32_t j[VLF];
 #pragma unroll
-    for (int w = 0; w < 4; w++) {
+    for (int w = 0; w < VLF; w++) {
       const uint32_t cw = c + (uint32_t)(w * GLF);
       j[w] = (cw < n) ? __ldg(&lst[(size_t)cw * NS]) : NO_RANK;
     }
-    float4 pj[4];
+    float4 pj[VLF];
 #pragma unroll
-    for (int w = 0; w < 4; w++) pj[w] = epos[(j[w] != NO_RANK) ? j[w] : j[0]];
+    for (int w = 0; w < VLF; w++) pj[w] = epos[(j[w] != NO_RANK) ? j[w] : j[0]];
 #pragma unroll
-    for (int w = 0; w < 4; w++) {
+    for (int w = 0; w < VLF; w++) {
       const float ex = pj[w].x - pi.x, ey = pj[w].y - pi.y, ez = pj[w].z - pi.z;
       const float d2 = dot3(ex, ey, ez, ex, ey, ez);
       const float q = 1.0f - approx_sqrt(d2) * invH;
@@ -233,12 +237,11 @@ __device__ __forceinline__ void vl_walk(const SimView& v, const CellHash& ch, in
 // by a ballot, so a list holds its candidates in walk order (deterministic
 // sums). At a rebuild a candidate's rank is its slot.
 __device__ __forceinline__ void vl_rebuild_one(const SimView& v, const DevParams* __restrict__ P, uint32_t r,
-                                               int lane, int g, uint32_t* __restrict__ lst, uint32_t& lcount) {
+                                               int lane, int g) {
   const unsigned FULL = 0xffffffffu;
   uint32_t i, myslot;
   bool act;
   vl_group(v, r, true, i, myslot, act);  // the same for every lane of the warp
-  lcount = 0;
   if (lane == 0 && r < (uint32_t)v.N) {  // the new rank order
     v.ep[r] = i;
     if (i != NO_RANK) v.erank[i] = r;
@@ -309,12 +312,15 @@ __device__ __forceinline__ void vl_rebuild_one(const SimView& v, const DevParams
   }
   const bool check = __any_sync(FULL, dup);
   const float4* __restrict__ spos = v.spos;
+  const uint32_t NS = (uint32_t)v.N;
+  uint32_t* __restrict__ lst = v.nbr + r;
   const unsigned lt = (1u << lane) - 1u;
-  auto place = [&](bool kp, uint32_t e) {  // into the warp's shared staging row
+  uint32_t lcount = 0;
+  auto place = [&](bool kp, uint32_t e) {
     const unsigned bal = __ballot_sync(FULL, kp);
     if (kp) {
       const uint32_t c = lcount + (uint32_t)__popc(bal & lt);
-      if (c < NLT) lst[c] = e;
+      if (c < NLT) lst[(size_t)c * NS] = e;
     }
     lcount += (uint32_t)__popc(bal);
   };
@@ -428,28 +434,10 @@ __device__ __forceinline__ void b_density_rebuild_vl(const SimView& v, const Dev
                                                      uint32_t vb) {
   if (v.scratch[SCR_REBUILD] == 0u) return;  // one value for the whole scene
   if (vb == 0 && threadIdx.x == 0) v.scratch[SCR_DIRTY] = 0u;
-  constexpr int RW = 32 / GLF;  // ranks per warp
-  __shared__ uint32_t s_lst[256 / 32][RW][NLT];  // each warp's lists before they are written out
-  const int lane = threadIdx.x & 31, w = (int)(threadIdx.x >> 5);
-  const int g = w * (32 / GLF);  // this warp's first walk-table row
-  const uint32_t r0 = (UPBD_VTID >> 5) * RW;
-  uint32_t cnt[RW];
-#pragma unroll
-  for (int k = 0; k < RW; k++) vl_rebuild_one(v, P, r0 + (uint32_t)k, lane, g, s_lst[w][k], cnt[k]);
-  __syncwarp();
-  // write out row by row: entry c of the warp's RW consecutive ranks is one
-  // run of RW words (lane: entry c0 + lane / RW of rank r0 + lane % RW)
-  uint32_t most = 0;
-#pragma unroll
-  for (int k = 0; k < RW; k++) most = max(most, min(cnt[k], NLT));
-  const int k = lane % RW;
-  const uint32_t NS = (uint32_t)v.N;
-  for (uint32_t c0 = 0; c0 < most; c0 += 32 / RW) {
-    const uint32_t c = c0 + (uint32_t)(lane / RW);
-    const uint32_t r = r0 + (uint32_t)k;
-    if (c < min(cnt[k], NLT) && r < NS) v.nbr[(size_t)c * NS + r] = s_lst[w][k][c];
-  }
-  __syncwarp();
+  const int lane = threadIdx.x & 31;
+  const int g = (int)(threadIdx.x >> 5) * (32 / GLF);  // this warp's first walk-table row
+  const uint32_t r0 = (UPBD_VTID >> 5) * (32 / GLF);
+  for (int k = 0; k < 32 / GLF; k++) vl_rebuild_one(v, P, r0 + (uint32_t)k, lane, g);
 }
 
 // fluidDensity (src/gpu/wgsl.js:254-279) on the substeps without a rebuild:
@@ -580,23 +568,23 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
     const uint32_t* __restrict__ lst = v.nbr + r;
     const float4* __restrict__ epos = v.epos;
     const float2* __restrict__ edens = v.edens;
-    for (uint32_t c = (uint32_t)lane; c < n; c += 4 * GLF) {  // four entries' loads in flight
-      uint32_t j[4];
+    for (uint32_t c = (uint32_t)lane; c < n; c += VLF * GLF) {  // VLF entries' loads in flight
+      uint32_t j[VLF];
 #pragma unroll
-      for (int w = 0; w < 4; w++) {
+      for (int w = 0; w < VLF; w++) {
         const uint32_t cw = c + (uint32_t)(w * GLF);
         j[w] = (cw < n) ? __ldg(&lst[(size_t)cw * NS]) : NO_RANK;
       }
-      float4 pj[4];
-      float2 dj[4];
+      float4 pj[VLF];
+      float2 dj[VLF];
 #pragma unroll
-      for (int w = 0; w < 4; w++) {
+      for (int w = 0; w < VLF; w++) {
         const uint32_t jj = (j[w] != NO_RANK) ? j[w] : j[0];
         pj[w] = epos[jj];
         dj[w] = edens[jj];
       }
 #pragma unroll
-      for (int w = 0; w < 4; w++)
+      for (int w = 0; w < VLF; w++)
         if (j[w] != NO_RANK) pair(pj[w], dj[w]);
     }
   }
@@ -699,22 +687,22 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
     const uint32_t* __restrict__ lst = v.nbr + r;
     const float4* __restrict__ epos = v.epos;
     const float4* __restrict__ evel = v.evel;
-    for (uint32_t c = (uint32_t)lane; c < n; c += 4 * GLF) {  // four entries' loads in flight
-      uint32_t j[4];
+    for (uint32_t c = (uint32_t)lane; c < n; c += VLF * GLF) {  // VLF entries' loads in flight
+      uint32_t j[VLF];
 #pragma unroll
-      for (int w = 0; w < 4; w++) {
+      for (int w = 0; w < VLF; w++) {
         const uint32_t cw = c + (uint32_t)(w * GLF);
         j[w] = (cw < n) ? __ldg(&lst[(size_t)cw * NS]) : NO_RANK;
       }
-      float4 pj[4], uj[4];
+      float4 pj[VLF], uj[VLF];
 #pragma unroll
-      for (int w = 0; w < 4; w++) {
+      for (int w = 0; w < VLF; w++) {
         const uint32_t jj = (j[w] != NO_RANK) ? j[w] : j[0];
         pj[w] = epos[jj];
         uj[w] = evel[jj];
       }
 #pragma unroll
-      for (int w = 0; w < 4; w++) {
+      for (int w = 0; w < VLF; w++) {
         const float ex = pj[w].x - pi.x, ey = pj[w].y - pi.y, ez = pj[w].z - pi.z;
         bool in = j[w] != NO_RANK && dot3(ex, ey, ez, ex, ey, ez) < H2;
         // a neighbour that changed cell after the grid build counts when its
