@@ -209,19 +209,71 @@ __device__ __forceinline__ void vl_density_list(const SimView& v, uint32_t r, in
   }
 }
 
-// Walk of the groups that cannot read their lists: where one or two groups
-// of a warp walk, all 32 lanes load their candidates for them in turn
-// (lane_staged); where more do, each walks its own share. Every lane of the
-// warp calls it.
-template <class Load, class Use>
-__device__ __forceinline__ void vl_walk(const SimView& v, const CellHash& ch, int lane, bool walks, Load&& load,
-                                        Use&& use) {
-  const unsigned wg = __ballot_sync(0xffffffffu, walks && lane == 0);
-  if (wg == 0u) return;
-  if (__popc(wg) <= 2)
-    lane_staged<0, GLF>(v, ch, lane, walks, load, use);
-  else
-    lane_strided<0, GLF>(v, ch, lane, walks, load, use);
+// Per-lane partial sums of a walk (K floats).
+template <int K>
+struct VAcc {
+  float v[K];
+};
+
+// Lane src's copy of x (a struct of 32-bit words).
+template <class T>
+__device__ __forceinline__ T vl_shfl(const T& x, int src) {
+  static_assert(sizeof(T) % 4 == 0, "32-bit fields only");
+  T y;
+  const uint32_t* a = reinterpret_cast<const uint32_t*>(&x);
+  uint32_t* b = reinterpret_cast<uint32_t*>(&y);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(T) / 4); k++) b[k] = __shfl_sync(0xffffffffu, a[k], src);
+  return y;
+}
+
+// Walk of the groups that cannot read their lists: all 32 lanes of the warp
+// walk each walking group's 27-bucket sequence in turn (candidate c to lane
+// c mod 32), with the group's own data `st` broadcast from its first lane;
+// term(st, e, load(e)) gives a candidate's contribution, and the warp's sum
+// is added to `out` on the group's first lane (the other lanes add nothing).
+// A walk then costs about seven steps instead of fifty, so the few particles
+// that walk do not hold the launch open. Every lane of the warp calls it.
+template <int K, class St, class Load, class Term>
+__device__ __forceinline__ void vl_walk(const SimView& v, const CellHash& ch, int lane, bool walks, const St& st,
+                                        Load&& load, Term&& term, VAcc<K>& out) {
+  const unsigned FULL = 0xffffffffu;
+  const unsigned todo0 = __ballot_sync(FULL, walks && lane == 0);  // one bit per walking group
+  if (todo0 == 0u) return;
+  const int L = (int)(threadIdx.x & 31), w = (int)(threadIdx.x >> 5);
+  const int g = w * (32 / GLF) + L / GLF;
+  walk_tables<0, GLF>(v, ch, lane, walks, g);
+  unsigned todo = todo0;
+  while (todo) {
+    const int first = __ffs(todo) - 1;  // the group's lane 0
+    todo &= todo - 1u;
+    const int gw = w * (32 / GLF) + first / GLF;
+    const St sw = vl_shfl(st, first);
+    const uint32_t run = s_walk_off[gw][27];
+    uint32_t k = 0, next = s_walk_off[gw][1], base = s_walk_base[gw][0];
+    VAcc<K> acc;
+#pragma unroll
+    for (int q = 0; q < K; q++) acc.v[q] = 0.f;
+    for (uint32_t c = (uint32_t)L; c < run; c += 32) {
+      while (c >= next) {
+        k++;
+        next = s_walk_off[gw][k + 1];
+        base = s_walk_base[gw][k];
+      }
+      const uint32_t e = base + c;
+      const VAcc<K> t = term(sw, e, load(e));
+#pragma unroll
+      for (int q = 0; q < K; q++) acc.v[q] = acc.v[q] + t.v[q];
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      float x = acc.v[q];
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) x = x + __shfl_xor_sync(FULL, x, d);
+      if (L == first) out.v[q] = out.v[q] + x;
+    }
+  }
+  __syncwarp();  // the next call may rewrite this warp's table rows
 }
 
 // fluidDensity (src/gpu/wgsl.js:254-279) at a rebuild for the particle of
@@ -478,16 +530,24 @@ __device__ __forceinline__ void b_density_vl(const SimView& v, const DevParams* 
   const bool walks = act && !listed;
   float rho = 0.f, rhoNear = 0.f;
   {
+    struct St {
+      float4 p;
+      uint32_t slot;
+    };
     const float4* __restrict__ spos = v.spos;
-    vl_walk(v, ch, lane, walks, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-      const bool in = (e != myslot) && (d2 < H2);
-      const float q = 1.0f - approx_sqrt(d2) * invH;
-      const float qq = in ? q * q : 0.0f;
-      rho = rho + qq;
-      rhoNear = rhoNear + qq * q;
-    });
+    VAcc<2> wsum = {{0.f, 0.f}};
+    vl_walk(v, ch, lane, walks, St{pi, myslot}, [&](uint32_t e) { return spos[e]; },
+            [&](const St& s, uint32_t e, const float4& pj) {
+              const float ex = pj.x - s.p.x, ey = pj.y - s.p.y, ez = pj.z - s.p.z;
+              const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+              const bool in = (e != s.slot) && (d2 < H2);
+              const float q = 1.0f - approx_sqrt(d2) * invH;
+              const float qq = in ? q * q : 0.0f;
+              return VAcc<2>{{qq, qq * q}};
+            },
+            wsum);
+    rho = rho + wsum.v[0];
+    rhoNear = rhoNear + wsum.v[1];
   }
   if (listed) vl_density_list(v, r, lane, pi, H2, invH, rho, rhoNear);
   rho = lane_sum<GLF>(rho);
@@ -556,11 +616,32 @@ __device__ __forceinline__ void b_disp_vl(const SimView& v, const DevParams* __r
       float4 p;
       float2 d;
     };
+    struct St {
+      float4 p;
+      uint32_t slot;
+      float Pi, PNi;
+    };
     const float4* __restrict__ spos = v.spos;
     const float2* __restrict__ sdens = v.sdens;
-    vl_walk(v, ch, lane, walks, [&](uint32_t e) { return PD{spos[e], sdens[e]}; }, [&](uint32_t e, const PD& c) {
-      if (e != myslot) pair(c.p, c.d);
-    });
+    VAcc<3> wsum = {{0.f, 0.f, 0.f}};
+    vl_walk(v, ch, lane, walks, St{pi, myslot, Pi, PNi}, [&](uint32_t e) { return PD{spos[e], sdens[e]}; },
+            [&](const St& s, uint32_t e, const PD& c) {
+              VAcc<3> t = {{0.f, 0.f, 0.f}};
+              const float ex = c.p.x - s.p.x, ey = c.p.y - s.p.y, ez = c.p.z - s.p.z;
+              const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+              if (e == s.slot || d2 >= H2 || d2 < 1e-12f) return t;
+              const float rd = rsqrtf(d2);
+              const float q = 1.0f - d2 * rd * invH;
+              const float Pj = k * (c.d.x - rho0);
+              const float PNj = kn * c.d.y;
+              float D = 0.25f * ((s.Pi + Pj) * q + (s.PNi + PNj) * q * q);
+              D = clampf(D, -maxPair, maxPair);
+              const float f = D * rd;
+              t.v[0] = -ex * f; t.v[1] = -ey * f; t.v[2] = -ez * f;
+              return t;
+            },
+            wsum);
+    sx = sx + wsum.v[0]; sy = sy + wsum.v[1]; sz = sz + wsum.v[2];
   }
   if (listed) {  // lane l reads entries l, l + GLF, ...
     const uint32_t NS = (uint32_t)v.N;
@@ -671,15 +752,21 @@ __device__ __forceinline__ void b_xsph_vl(const SimView& v, const DevParams* __r
     struct PV {
       float4 p, v;
     };
+    struct St {
+      float4 p;
+      uint32_t slot;
+    };
     const float4* __restrict__ spos = v.spos;
     const float4* __restrict__ svel = v.svel;
-    vl_walk(v, ch, lane, walks, [&](uint32_t e) { return PV{spos[e], svel[e]}; },
-                         [&](uint32_t e, const PV& c) {
-                           const float ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
-                           const bool in = (e != myslot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
-                           sx = sx + (in ? c.v.x : 0.f); sy = sy + (in ? c.v.y : 0.f);
-                           sz = sz + (in ? c.v.z : 0.f); m = m + (in ? 1.0f : 0.f);
-                         });
+    VAcc<4> wsum = {{0.f, 0.f, 0.f, 0.f}};
+    vl_walk(v, ch, lane, walks, St{pi, myslot}, [&](uint32_t e) { return PV{spos[e], svel[e]}; },
+            [&](const St& s, uint32_t e, const PV& c) {
+              const float ex = c.p.x - s.p.x, ey = c.p.y - s.p.y, ez = c.p.z - s.p.z;
+              const bool in = (e != s.slot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
+              return VAcc<4>{{in ? c.v.x : 0.f, in ? c.v.y : 0.f, in ? c.v.z : 0.f, in ? 1.0f : 0.f}};
+            },
+            wsum);
+    sx = sx + wsum.v[0]; sy = sy + wsum.v[1]; sz = sz + wsum.v[2]; m = m + wsum.v[3];
   }
   if (listed) {  // lane l reads entries l, l + GLF, ...
     const uint32_t NS = (uint32_t)v.N;
