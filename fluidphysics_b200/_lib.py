@@ -66,12 +66,6 @@ class Info(C.Structure):
     ]
 
 
-class ListInfo(C.Structure):
-    """upbd_list_info (include/upbd.h)."""
-    _fields_ = [("rebuilds", C.c_uint64), ("walkers", C.c_uint32), ("listed", C.c_uint32),
-                ("complete", C.c_uint32), ("max_len", C.c_uint32), ("mean_len", C.c_double)]
-
-
 class DevicePtrs(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in ("pos", "prev", "vel", "density", "flags", "cons", "stream")]
 
@@ -177,7 +171,6 @@ _SIGS = [
     ("upbd_write_tets", C.c_int, [_P, _U]),
     ("upbd_set_fluid_next", C.c_int, [_P, C.c_int32]),
     ("upbd_groups", C.c_int, [_P, C.POINTER(C.c_int32)]),
-    ("upbd_list_stats", C.c_int, [_P, _P]),
     ("upbd_grid_build", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
     ("upbd_grid_build_noalloc", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
     ("upbd_launch_count", C.c_uint64, [_P]),

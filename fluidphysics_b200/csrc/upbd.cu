@@ -154,14 +154,6 @@ cudaEvent_t prof_event(upbd_sim* s) {
 
 void fill_static_params(upbd_sim* s) { fill_dev_params(s->prm, s->desc, s->hp); }
 
-// The product build's fluid neighbour lists no longer describe the state (a
-// state write, an emit, a drain, new constants): the next substep rebuilds
-// them. Stream-ordered, so it lands before that substep.
-int lists_stale(upbd_sim* s) {
-  UPBD_CK(s, cudaMemsetAsync(s->v.scratch + SCR_DIRTY, 0xff, sizeof(uint32_t), s->stream));
-  return UPBD_OK;
-}
-
 int upload_params(upbd_sim* s) {
   const int k = s->stage_next;
   s->stage_next = (k + 1) % kStageRing;
@@ -214,7 +206,7 @@ int launch_substep(upbd_sim* s, int last) {
   }
   PROF(s, K_SCAN, k_scan<<<v.num_tiles, SCAN_THREADS, 0, st>>>(v));
   PROF(s, K_SCATTER, k_scatter<<<blocks_for(std::max(v.N, tile_words(v.num_tiles))), 256, 0, st>>>(v));
-  PROF(s, K_RANKFIX, k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v, P));
+  PROF(s, K_RANKFIX, k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v));
   L += 4;
   UPBD_KCK(s);
   if (overlap) {
@@ -226,19 +218,13 @@ int launch_substep(upbd_sim* s, int last) {
   }
   if (last < UPBD_PASS_DENSITY) return UPBD_OK;
   const long long fl = (long long)v.N * GLF;  // lane-parallel fluid gathers over the slots
-#ifndef UPBD_PARITY_BUILD
-  // a rebuild substep's density (lists, rank order) in a launch of its own,
-  // so the list launch keeps few registers; each returns on the other's substeps
-  PROF(s, K_DENSITY, k_density_rebuild<<<blocks_for(fl), 256, 0, st>>>(v, P));
-  L++;
-#endif
   PROF(s, K_DENSITY, k_density<<<blocks_for(fl), 256, 0, st>>>(v, P));
   L++;
   if (last < UPBD_PASS_DISP) return UPBD_OK;
-  if (fold)  // DISP_LANES threads per slot
-    PROF(s, K_DISP, k_disp<true><<<blocks_for((long long)v.N * DISP_LANES), 256, 0, st>>>(v, P));
+  if (fold)  // DL threads per slot
+    PROF(s, K_DISP, k_disp<true><<<blocks_for((long long)v.N * DL), 256, 0, st>>>(v, P));
   else
-    PROF(s, K_DISP, k_disp<false><<<blocks_for((long long)v.N * DISP_LANES), 256, 0, st>>>(v, P));
+    PROF(s, K_DISP, k_disp<false><<<blocks_for((long long)v.N * DL), 256, 0, st>>>(v, P));
   L++;
   UPBD_KCK(s);
   if (last < UPBD_PASS_APPLY_FLUID) return UPBD_OK;
@@ -325,12 +311,7 @@ int launch_substep(upbd_sim* s, int last) {
     L++;
     return UPBD_OK;
   }
-#ifdef UPBD_PARITY_BUILD
-  const bool xsph_split = !s->prof_on && s->side;
-#else
-  const bool xsph_split = false;  // lists: few groups walk, one launch
-#endif
-  if (xsph_split) {
+  if (!s->prof_on && s->side) {
     // xsph as two launches side by side: the groups that walk on the side
     // stream (its launch first, so its long warps start early) and those that
     // read their lists on the main stream, each launch with the registers its
@@ -640,7 +621,6 @@ int upbd_set_params(upbd_sim* s, const upbd_params* p) {
   cudaSetDevice(s->device);
   s->prm = *p;
   fill_static_params(s);
-  if (int rc = lists_stale(s)) return rc;
   return upload_params(s);
 }
 
@@ -750,7 +730,6 @@ int upbd_reset_solid(upbd_sim* s) {
     UPBD_CK(s, cudaMemcpyAsync(v.cons, s->init_cons.data(), (size_t)v.C * 16, cudaMemcpyHostToDevice, st));
   if (v.NT > 0)
     UPBD_CK(s, cudaMemcpyAsync(v.tet_vol, s->init_tet_vol.data(), (size_t)v.NT * 4, cudaMemcpyHostToDevice, st));
-  if (int rc = lists_stale(s)) return rc;
   UPBD_CK(s, cudaStreamSynchronize(st));
   return UPBD_OK;
 }
@@ -763,7 +742,7 @@ int upbd_drain(upbd_sim* s) {
     s->launches++;
     UPBD_KCK(s);
   }
-  return lists_stale(s);
+  return UPBD_OK;
 }
 
 int upbd_active_count(upbd_sim* s, uint32_t* count) {
@@ -807,7 +786,6 @@ int upbd_emit_particles(upbd_sim* s, int32_t n, const float* pos3, const float* 
   s->launches++;
   UPBD_KCK(s);
   UPBD_CK(s, cudaFreeAsync(dbuf, s->stream));
-  if (int rc = lists_stale(s)) return rc;
   UPBD_CK(s, cudaStreamSynchronize(s->stream));
   s->fluid_next = (int)(((long long)s->fluid_next + n) % s->v.F);
   return UPBD_OK;
@@ -1005,7 +983,6 @@ int upbd_write_state(upbd_sim* s, const float* pos4, const float* prev4, const f
   if (vel4) UPBD_CK(s, cudaMemcpyAsync(s->v.vel, vel4, N * 16, cudaMemcpyHostToDevice, st));
   if (density2) UPBD_CK(s, cudaMemcpyAsync(s->v.density, density2, N * 8, cudaMemcpyHostToDevice, st));
   if (flags) UPBD_CK(s, cudaMemcpyAsync(s->v.flags, flags, N * 4, cudaMemcpyHostToDevice, st));
-  if (int rc = lists_stale(s)) return rc;
   UPBD_CK(s, cudaStreamSynchronize(st));
   return UPBD_OK;
 }
@@ -1069,7 +1046,7 @@ int upbd_rebuild_grid(upbd_sim* s) {
   k_integrate_count<false, true><<<blocks_for(v.N), 256, 0, st>>>(v, s->dparams);
   k_scan<<<v.num_tiles, SCAN_THREADS, 0, st>>>(v);
   k_scatter<<<blocks_for(std::max(v.N, tile_words(v.num_tiles))), 256, 0, st>>>(v);
-  k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v, s->dparams);
+  k_rankfix<<<blocks_for(v.N), 256, 0, st>>>(v);
   s->launches += 4;
   UPBD_KCK(s);
   UPBD_CK(s, cudaStreamSynchronize(st));
@@ -1238,37 +1215,11 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
   k_integrate_count<false, true><<<blocks_for(n), 256, 0, st>>>(v, dp);
   k_scan<<<tiles, SCAN_THREADS, 0, st>>>(v);
   k_scatter<<<blocks_for(std::max(n, tile_words(tiles))), 256, 0, st>>>(v);
-  k_rankfix<<<blocks_for(n), 256, 0, st>>>(v, dp);
+  k_rankfix<<<blocks_for(n), 256, 0, st>>>(v);
   // counts[h] = offsets[h+1] - offsets[h] (the scan cleared its own counts)
   if (counts) k_counts_from_offsets<<<blocks_for(table_size), 256, 0, st>>>(v.start, (uint32_t*)counts, table_size);
   cudaError_t e = cudaPeekAtLastError();
   if (e != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, cudaGetErrorString(e));
-  return UPBD_OK;
-}
-
-int upbd_list_stats(upbd_sim* s, upbd_list_info* out) {
-  if (!s || !out) return UPBD_ERR_INVALID;
-  cudaSetDevice(s->device);
-  std::memset(out, 0, sizeof(*out));
-#ifndef UPBD_PARITY_BUILD
-  UPBD_CK(s, cudaMemsetAsync(s->v.scratch + SCR_CENSUS, 0, 4 * sizeof(uint32_t), s->stream));
-  if (s->v.F > 0) {
-    k_list_census<<<blocks_for(s->v.F), 256, 0, s->stream>>>(s->v);
-    UPBD_KCK(s);
-  }
-  uint32_t w[SCR_WORDS];
-  UPBD_CK(s, cudaMemcpyAsync(w, s->v.scratch, sizeof(w), cudaMemcpyDeviceToHost, s->stream));
-  UPBD_CK(s, cudaStreamSynchronize(s->stream));
-  uint32_t act = 0;
-  int rc = upbd_active_count(s, &act);
-  if (rc) return rc;
-  out->rebuilds = w[SCR_REBUILDS];
-  out->walkers = w[SCR_WALKERS];
-  out->listed = w[SCR_CENSUS];
-  out->complete = w[SCR_CENSUS + 1];
-  out->max_len = w[SCR_CENSUS + 2];
-  out->mean_len = act ? (double)w[SCR_CENSUS + 3] / act : 0.0;
-#endif
   return UPBD_OK;
 }
 
@@ -1387,7 +1338,7 @@ extern "C" int upbd_grid_build_noalloc(const void* pos4, const void* flags, int3
   k_integrate_count<false, true><<<blocks_for(n), 256, 0, st>>>(v, dp);
   k_scan<<<tiles, SCAN_THREADS, 0, st>>>(v);
   k_scatter<<<blocks_for(std::max(n, tile_words(tiles))), 256, 0, st>>>(v);
-  k_rankfix<<<blocks_for(n), 256, 0, st>>>(v, dp);
+  k_rankfix<<<blocks_for(n), 256, 0, st>>>(v);
   if (counts) k_counts_from_offsets<<<blocks_for(table_size), 256, 0, st>>>(v.start, (uint32_t*)counts, table_size);
   e = cudaPeekAtLastError();
   if (e != cudaSuccess) return fail(nullptr, UPBD_ERR_CUDA, cudaGetErrorString(e));

@@ -40,7 +40,7 @@ enum Domain {
   D_TILES,    // scan tiles of the bucket table (SCAN_THREADS per block)
   D_SCATTER,  // max(particles, scan tiles)
   D_FGL,      // GLF lanes per grid slot (density, xsph)
-  D_DISP,     // DISP_LANES threads per grid slot (displacement)
+  D_DISP,     // DL threads per grid slot (displacement)
   D_F,        // fluid particles (apply, xsph apply, active count)
   D_SOLVE0,   // solve lanes rounded to warps + fluid (first iteration)
   D_SOLVE,    // solve lanes rounded to warps
@@ -114,29 +114,16 @@ __global__ void __launch_bounds__(256) kb_scatter(BatchArgs a) {
   batch_loop<D_SCATTER, false>(a, UPBD_BODY { b_scatter(v, vb); });
 }
 __global__ void __launch_bounds__(256) kb_rankfix(BatchArgs a) {
-  batch_loop<D_N, false, true>(a, UPBD_BODY { b_rankfix(v, P, vb); });
+  batch_loop<D_N, false, true>(a, UPBD_BODY { b_rankfix(v, vb); });
 }
 // density and the solve are latency-bound: at most 40 registers (6 CTAs of
 // 256 per SM) hides more of it than the few spilled values cost
 __global__ void __launch_bounds__(256, 6) kb_density(BatchArgs a) {
-#ifdef UPBD_PARITY_BUILD
   batch_loop<D_FGL, false, true>(a, UPBD_BODY { b_density(v, P, vb); });
-#else
-  batch_loop<D_FGL, false, true>(a, UPBD_BODY { b_density_vl(v, P, vb); });
-#endif
 }
-#ifndef UPBD_PARITY_BUILD
-__global__ void __launch_bounds__(256) kb_density_rebuild(BatchArgs a) {
-  batch_loop<D_FGL, false, true>(a, UPBD_BODY { b_density_rebuild_vl(v, P, vb); });
-}
-#endif
 template <bool APPLY>
 __global__ void __launch_bounds__(256) kb_disp(BatchArgs a) {
-#ifdef UPBD_PARITY_BUILD
   batch_loop<D_DISP, false>(a, UPBD_BODY { b_disp<APPLY>(v, P, vb); });
-#else
-  batch_loop<D_DISP, false>(a, UPBD_BODY { b_disp_vl<APPLY>(v, P, vb); });
-#endif
 }
 __global__ void __launch_bounds__(256) kb_apply_fluid(BatchArgs a) {
   batch_loop<D_F, false>(a, UPBD_BODY { b_apply_fluid(v, vb); });
@@ -185,11 +172,7 @@ __global__ void __launch_bounds__(256) kb_solid_visc_apply(BatchArgs a) {
   });
 }
 __global__ void __launch_bounds__(256) kb_xsph(BatchArgs a) {
-#ifdef UPBD_PARITY_BUILD
   batch_loop<D_FGL, false>(a, UPBD_BODY { b_xsph<true>(v, P, vb); });
-#else
-  batch_loop<D_FGL, false>(a, UPBD_BODY { b_xsph_vl<true>(v, P, vb); });
-#endif
 }
 __global__ void __launch_bounds__(256) kb_count_active(BatchArgs a) {
   batch_loop<D_F, true>(a, UPBD_BODY { b_count_active(v, vb, nblk); });
@@ -211,7 +194,7 @@ void scene_blocks(const SimView& v, bool tets, int bt, uint32_t out[NUM_DOMAINS]
   out[D_TILES] = (uint32_t)std::max(v.num_tiles, 1);
   out[D_SCATTER] = ceil_div(std::max(v.N, tile_words(v.num_tiles)), bt);
   out[D_FGL] = ceil_div((long long)v.N * GLF, bt);
-  out[D_DISP] = ceil_div((long long)v.N * DISP_LANES, bt);
+  out[D_DISP] = ceil_div((long long)v.N * DL, bt);
   out[D_F] = ceil_div(v.F, bt);
   out[D_SOLVE0] = ceil_div((long long)sp + v.F, bt);
   out[D_SOLVE] = ceil_div(sp, bt);
@@ -453,9 +436,6 @@ int launch_batch_frame(upbd_batch* b, int nsub, bool visc) {
     BLAUNCH(b, K_SCAN, kb_scan<<<G, SCAN_THREADS, 0, st>>>(a));
     BLAUNCH(b, K_SCATTER, kb_scatter<<<G, BT, 0, st>>>(a));
     BLAUNCH(b, K_RANKFIX, kb_rankfix<<<G, BT, 0, st>>>(a));
-#ifndef UPBD_PARITY_BUILD
-    BLAUNCH(b, K_DENSITY, kb_density_rebuild<<<G, BT, 0, st>>>(a));  // returns at once without a rebuild
-#endif
     BLAUNCH(b, K_DENSITY, kb_density<<<G, BT, 0, st>>>(a));
     if (fold)  // the displacement pass applies the fluid's move (b_disp<true>)
       BLAUNCH(b, K_DISP, kb_disp<true><<<G, BT, 0, st>>>(a));
@@ -772,8 +752,6 @@ int upbd_batch_set_params(upbd_batch* b, int32_t id, const upbd_params* p) {
   fill_dev_params(*p, sc->desc, sc->hp);
   sc->hp.grab_lattice = 0xffff;
   b->dirty = true;
-  cudaSetDevice(b->device);
-  BCK(b, cudaMemsetAsync(sc->v.scratch + SCR_DIRTY, 0xff, sizeof(uint32_t), b->stream));  // new H or cell size
   return UPBD_OK;
 }
 
@@ -849,8 +827,6 @@ int upbd_batch_write_state(upbd_batch* b, int32_t id, const float* pos4, const f
   if (vel4) BCK(b, cudaMemcpyAsync(sc->v.vel, vel4, N * 16, cudaMemcpyHostToDevice, st));
   if (density2) BCK(b, cudaMemcpyAsync(sc->v.density, density2, N * 8, cudaMemcpyHostToDevice, st));
   if (flags) BCK(b, cudaMemcpyAsync(sc->v.flags, flags, N * 4, cudaMemcpyHostToDevice, st));
-  // the product build's fluid lists are rebuilt at the next substep
-  BCK(b, cudaMemsetAsync(sc->v.scratch + SCR_DIRTY, 0xff, sizeof(uint32_t), st));
   BCK(b, cudaStreamSynchronize(st));
   return UPBD_OK;
 }

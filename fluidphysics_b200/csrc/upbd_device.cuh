@@ -32,13 +32,7 @@ constexpr int SCR_CUT = 3;         // constraints cut by the last wedge
 constexpr int SCR_ACTIVE = 4;      // active-fluid partial sums
 constexpr int SCR_DONE = 5;        // blocks finished (last-block pattern)
 constexpr int SCR_HEALTH = 6;      // UPBD_HEALTH_* bits
-constexpr int SCR_XMOVE = 7;       // largest movement the bounds pass recorded this substep (float bits;
-                                   // product build: of the particles below VFAST)
-constexpr int SCR_REBUILD = 8;     // product build: this substep's density pass rebuilds every fluid list
-constexpr int SCR_DIRTY = 9;       // product build: the lists no longer describe the state (set by tools, culls)
-constexpr int SCR_WALKERS = 10;    // product build: particles that walked for want of a usable list this substep
-constexpr int SCR_REBUILDS = 11;   // product build: substeps that rebuilt the lists (wraps at 2^32)
-constexpr int SCR_CENSUS = 12;     // product build: list census (listed, complete, longest, total length)
+constexpr int SCR_XMOVE = 7;       // largest movement the bounds pass recorded this substep (float bits)
 constexpr int SCR_WORDS = 16;
 // mapped host words
 constexpr int HM_ACTIVE = 0;
@@ -61,10 +55,7 @@ struct DevParams {
   // 1 when solid_radius + fluid_radius is below the cell size: every
   // solid↔fluid contact then lies in adjacent cells, so the solids can mark
   // the fluid particles that have one and the rest skip their gather.
-  int32_t use_mark;
-  // 1 when the fluid gathers may keep neighbour lists across substeps
-  // (fluid_h at most the cell size; product build only)
-  int32_t use_lists;
+  int32_t use_mark, pad4;
   float4 grab_delta;  // per-substep share of the frame's grab motion
   uint32_t emit_count, emit_start, grab_lattice, pad3;
   float4 emit_pos, emit_dir, emit_side, emit_up;
@@ -126,31 +117,6 @@ struct SimView {
   float4* sfp;
   uint32_t* ccount;
   uint32_t* clist;
-  // Product build: fluid neighbour lists kept across substeps. They live in
-  // the "rank" order of the last rebuild (the grid's slot order at that
-  // substep, so neighbours sit close together): ep[r] is the particle of
-  // rank r (NO_RANK past the active ones), erank[i] the rank of particle i.
-  // The list of rank r holds ranks, nbr[c * N + r] for c < ncount[r] <= NLT
-  // (reusing the parity build's per-substep list arrays), and xlist[r] is the
-  // position it was built at. The gathers read their neighbours from
-  // rank-ordered copies: epos (grid-time positions, then from the bounds
-  // pass on the final ones), edens (density) and evel (velocity after the
-  // velocity pass; w = 1 when the particle changed cell after the grid
-  // build). pfl holds per-particle state bits (PF_* below); bfast marks the
-  // buckets around particles that moved far since the rebuild (cleared by
-  // the scan every substep).
-  uint32_t* ep;
-  uint32_t* erank;
-  // per rank {particle, slot, grid bucket, state bits}: written by the rank
-  // fix-up (a rebuild: the density pass), the state bits updated by the
-  // density and bounds passes; the gathers start from it with one load
-  uint4* erec;
-  float4* xlist;
-  float4* epos;
-  float2* edens;
-  float4* evel;
-  uint32_t* pfl;
-  uint32_t* bfast;
   uint32_t* scratch;
   uint32_t* host_mapped;
   int S, N1, dim1, dim2, F, N, C, NT, T, num_tiles;
@@ -199,31 +165,6 @@ struct CellHash {
   }
 };
 
-// True when two of the 27 cells around the cell of CellHash ch share a hash
-// bucket. Cells (a,b,c) and (a',b',c') collide exactly when
-// (X_a^X_a') ^ (Y_b^Y_b') ^ (Z_c^Z_c') is 0 under the mask, so the test runs
-// over the 4 x 4 x 4 choices of equal (0) or one of three pair differences
-// per axis, all but the all-equal one.
-__device__ __forceinline__ bool buckets_coincide(const CellHash& ch, uint32_t mask) {
-  const uint32_t dx[4] = {0u, (uint32_t)(ch.hx[0] ^ ch.hx[1]) & mask, (uint32_t)(ch.hx[0] ^ ch.hx[2]) & mask,
-                          (uint32_t)(ch.hx[1] ^ ch.hx[2]) & mask};
-  const uint32_t dy[4] = {0u, (uint32_t)(ch.hy[0] ^ ch.hy[1]) & mask, (uint32_t)(ch.hy[0] ^ ch.hy[2]) & mask,
-                          (uint32_t)(ch.hy[1] ^ ch.hy[2]) & mask};
-  const uint32_t dz[4] = {0u, (uint32_t)(ch.hz[0] ^ ch.hz[1]) & mask, (uint32_t)(ch.hz[0] ^ ch.hz[2]) & mask,
-                          (uint32_t)(ch.hz[1] ^ ch.hz[2]) & mask};
-  bool hit = false;
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const uint32_t xy = dx[a] ^ dy[b];
-#pragma unroll
-      for (int c = 0; c < 4; c++)
-        if (a | b | c) hit |= (xy == dz[c]);
-    }
-  return hit;
-}
-
 // Neighbour gathers run G lanes per particle (lane_strided below deals the
 // candidates to the lanes); each lane accumulates its own partial sums from
 // zero and the G partials are combined by a fixed xor butterfly, so the
@@ -235,16 +176,7 @@ __device__ __forceinline__ bool buckets_coincide(const CellHash& ch, uint32_t ma
 constexpr int GL = 8;
 constexpr int GLF = 4;
 constexpr uint32_t NL = 32;  // density-pass neighbour-list entries kept per fluid lane (GLF * NL per particle)
-constexpr uint32_t NLT = NL * GLF;  // product build: entries of one fluid particle's list kept across substeps
 constexpr int DL = 2;        // threads per particle in the displacement pass
-// threads per grid slot of the displacement launch: the parity build's DL
-// threads over the density pass's per-substep lists, the product build's GLF
-// lanes over its lane lists
-#ifdef UPBD_PARITY_BUILD
-constexpr int DISP_LANES = DL;
-#else
-constexpr int DISP_LANES = GLF;
-#endif
 
 // xsph sums over the fluid candidates within H at its own time, after the
 // displacement, contact and bounds passes moved the fluid. The density pass
@@ -262,37 +194,6 @@ constexpr float XSKIN = 0.05f;
 constexpr float XMOVE_FRAC = 0.9f;
 constexpr float XMOVE_REC = 0.25f;
 constexpr uint32_t NBR_IN = 0x80000000u;  // list entry flag: within H at density time (slots stay below 2^31)
-
-// Product build: neighbour lists kept across substeps (Verlet lists). At a
-// rebuild the density pass lists every fluid particle within H * (1 + VSKIN)
-// (the 27 cells and the cells beyond them that the radius reaches) and
-// records the particle's position. A later
-// substep may read the list instead of walking the 27 buckets when the
-// particle's own movement since the rebuild plus the largest movement of any
-// particle that can be within H of it stays within VMOVE_FRAC of the skin
-// (the rest covers rounding): then every fluid particle within H is listed.
-// Movements at or below VMOVE_REC * the allowance are not recorded per
-// bucket: a bucket counts them as that much.
-constexpr float VSKIN = 0.15f;
-constexpr float VMOVE_FRAC = 0.9f;
-constexpr float VMOVE_REC = 0.25f;
-// A particle that moved more than VFAST * the allowance since the rebuild
-// marks the 27 buckets around its cell (bfast) instead of raising the
-// scene-wide bound SCR_XMOVE, so a few fast particles send only their
-// neighbours to the per-bucket test.
-constexpr float VFAST = 0.5f;
-constexpr uint32_t NO_RANK = 0xffffffffu;
-// pfl bits
-constexpr uint32_t PF_DUP = 1u;    // two of the 27 buckets around the grid-time cell coincide
-constexpr uint32_t PF_DUPF = 2u;   // the same for the cell at xsph time
-constexpr uint32_t PF_LOK = 4u;    // the list is complete (it did not overflow at the rebuild)
-constexpr uint32_t PF_LIST = 8u;   // this substep's density and displacement read the list
-constexpr uint32_t PF_MOVED = 16u; // the particle changed cell after this substep's grid build
-constexpr uint32_t PF_CULLED = 32u; // (rank record only) culled by this substep's bounds pass
-// A rebuild follows a substep whose density and xsph passes walked, for want
-// of a usable list, for more than F / VWALK_DIV particles (walkers sit
-// together in rank order, so a few hundred cost little).
-constexpr uint32_t VWALK_DIV = 64u;
 
 template <int G = GL>
 __device__ __forceinline__ float lane_sum(float x) {

@@ -13,9 +13,6 @@ namespace upbd {
 __global__ void __launch_bounds__(64) k_emit(SimView v, const DevParams* __restrict__ P) {
   const uint32_t k = UPBD_TID;
   if (k >= P->emit_count) return;
-#ifndef UPBD_PARITY_BUILD
-  if (k == 0) v.scratch[SCR_DIRTY] = 1u;  // new particles: the fluid lists are rebuilt
-#endif
   const int slot = v.S + (int)((P->emit_start + k) % (uint32_t)v.F);
   const float4 E_pos = P->emit_pos, E_dir = P->emit_dir, E_side = P->emit_side, E_up = P->emit_up;
   const float phase = E_dir.w + (float)k * 2.39996f;
@@ -63,38 +60,13 @@ __global__ void __launch_bounds__(256) k_integrate_count(SimView v, const DevPar
 }
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(SimView v) { b_scan(v, blockIdx.x); }
 __global__ void __launch_bounds__(256) k_scatter(SimView v) { b_scatter(v, blockIdx.x); }
-__global__ void __launch_bounds__(256) k_rankfix(SimView v, const DevParams* __restrict__ P) {
-  b_rankfix(v, P, blockIdx.x);
-}
-#ifndef UPBD_PARITY_BUILD
-// Product build: a rebuild substep's density pass (returns at once on the
-// others, where k_density runs over the lists instead).
-__global__ void __launch_bounds__(256, 4) k_density_rebuild(SimView v, const DevParams* __restrict__ P) {
-  b_density_rebuild_vl(v, P, blockIdx.x);
-}
-#endif
-// The fluid gathers: the bucket walks in the parity build (the oracle's
-// summation order), lists kept across substeps in the product build (at 32
-// registers: eight blocks per SM, so a scene's groups are resident at once).
-#ifdef UPBD_PARITY_BUILD
-#define UPBD_GATHER_BOUNDS __launch_bounds__(256)
-#else
-#define UPBD_GATHER_BOUNDS __launch_bounds__(256, 8)
-#endif
-__global__ void UPBD_GATHER_BOUNDS k_density(SimView v, const DevParams* __restrict__ P) {
-#ifdef UPBD_PARITY_BUILD
+__global__ void __launch_bounds__(256) k_rankfix(SimView v) { b_rankfix(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_density(SimView v, const DevParams* __restrict__ P) {
   b_density(v, P, blockIdx.x);
-#else
-  b_density_vl(v, P, blockIdx.x);
-#endif
 }
 template <bool APPLY>
-__global__ void UPBD_GATHER_BOUNDS k_disp(SimView v, const DevParams* __restrict__ P) {
-#ifdef UPBD_PARITY_BUILD
+__global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __restrict__ P) {
   b_disp<APPLY>(v, P, blockIdx.x);
-#else
-  b_disp_vl<APPLY>(v, P, blockIdx.x);
-#endif
 }
 __global__ void __launch_bounds__(256) k_apply_fluid(SimView v) { b_apply_fluid(v, blockIdx.x); }
 template <bool APPLY_FLUID, int OUT>
@@ -133,12 +105,8 @@ __global__ void __launch_bounds__(256) k_solid_visc(SimView v, const DevParams* 
 }
 __global__ void __launch_bounds__(256) k_solid_visc_apply(SimView v) { b_solid_visc_apply(v, blockIdx.x); }
 template <bool APPLY, int ROLE = 0>
-__global__ void UPBD_GATHER_BOUNDS k_xsph(SimView v, const DevParams* __restrict__ P) {
-#ifdef UPBD_PARITY_BUILD
+__global__ void __launch_bounds__(256) k_xsph(SimView v, const DevParams* __restrict__ P) {
   b_xsph<APPLY, ROLE>(v, P, blockIdx.x);
-#else
-  b_xsph_vl<APPLY>(v, P, blockIdx.x);
-#endif
 }
 __global__ void __launch_bounds__(256) k_count_active(SimView v) { b_count_active(v, blockIdx.x, gridDim.x); }
 
@@ -298,34 +266,6 @@ __global__ void k_grab_indices(SimView v, const uint32_t* __restrict__ idx, cons
 __global__ void k_grab_release(SimView v) {
   const int i = UPBD_TID;
   if (i < v.S) v.flags[i] &= ~F_GRABBED;
-}
-
-// Census of the product build's fluid lists into scratch[SCR_CENSUS..+3]
-// (cleared by the caller): particles that read their list in the last
-// density pass, particles holding a complete list, the longest list, the
-// total length.
-__global__ void k_list_census(SimView v) {
-  const int i = v.S + (int)UPBD_TID;
-  uint32_t listed = 0, complete = 0, len = 0;
-  if (i < v.N && (v.flags[i] & F_ACTIVE) && v.pfl) {
-    const uint32_t r = v.erank[i];
-    if (r < (uint32_t)v.N) {
-      const uint32_t pf = v.erec[r].w;
-      listed = (pf & PF_LIST) ? 1u : 0u;
-      complete = (pf & PF_LOK) ? 1u : 0u;
-      len = v.ncount[r];
-    }
-  }
-  listed = __reduce_add_sync(0xffffffffu, listed);
-  complete = __reduce_add_sync(0xffffffffu, complete);
-  const uint32_t mx = __reduce_max_sync(0xffffffffu, len);
-  len = __reduce_add_sync(0xffffffffu, len);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&v.scratch[SCR_CENSUS], listed);
-    atomicAdd(&v.scratch[SCR_CENSUS + 1], complete);
-    atomicMax(&v.scratch[SCR_CENSUS + 2], mx);
-    atomicAdd(&v.scratch[SCR_CENSUS + 3], len);
-  }
 }
 
 // GpuSim.clearFluid, src/gpu/sim.js:294-297

@@ -23,17 +23,6 @@ namespace upbd {
 // and bumps its scan tile's total, so the scan needs no second pass.
 template <bool INTEGRATE, bool COUNT>
 __device__ __forceinline__ void b_integrate_count(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
-#ifndef UPBD_PARITY_BUILD
-  // the substep's list decision: rebuild after changes the lists cannot
-  // follow, or when the last substep walked for too many particles
-  if (INTEGRATE && COUNT && v.pfl && vb == 0 && threadIdx.x == 0) {
-    const uint32_t w = v.scratch[SCR_WALKERS];
-    const bool rb = P->use_lists && (v.scratch[SCR_DIRTY] != 0u || w > (uint32_t)v.F / VWALK_DIV);
-    v.scratch[SCR_REBUILD] = rb ? 1u : 0u;
-    v.scratch[SCR_WALKERS] = 0u;
-    if (rb) v.scratch[SCR_REBUILDS] += 1u;
-  }
-#endif
   const int i = UPBD_VTID;
   if (i >= v.N) return;
   uint32_t f = v.flags[i];
@@ -86,15 +75,6 @@ __device__ __forceinline__ void b_integrate_count(const SimView& v, const DevPar
   if (COUNT) {
     const uint32_t h = cell_of(p4.x, p4.y, p4.z, P->inv_cell, (uint32_t)v.T - 1u);
     v.cell[i] = h;
-#ifndef UPBD_PARITY_BUILD
-    if (v.pfl && i >= v.S) {  // whether the 27 buckets of this cell coincide (list rule)
-      CellHash ch;
-      ch.init(p4.x, p4.y, p4.z, P->inv_cell);
-      const bool dup = buckets_coincide(ch, (uint32_t)v.T - 1u);
-      const uint32_t pf = v.pfl[i];
-      v.pfl[i] = dup ? (pf | PF_DUP) : (pf & ~PF_DUP);
-    }
-#endif
     v.ticket[i] = atomicAdd(&v.counts[h], 1u);
     const int rep = (i >> 5) & (tile_reps(v.num_tiles) - 1);  // a power of two
     atomicAdd(&v.tile_sum[rep * v.num_tiles + (int)(h / SCAN_TILE)], 1u);
@@ -178,12 +158,6 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
       *reinterpret_cast<uint4*>(v.bmove + t0) = z;
       *reinterpret_cast<uint4*>(v.bmove + t0 + 4) = z;
     }
-#ifndef UPBD_PARITY_BUILD
-    if (v.bfast) {
-      *reinterpret_cast<uint4*>(v.bfast + t0) = z;
-      *reinterpret_cast<uint4*>(v.bfast + t0 + 4) = z;
-    }
-#endif
   } else {
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -193,9 +167,6 @@ __device__ __forceinline__ void b_scan(const SimView& v, uint32_t vb) {
         if (v.fend) v.fend[idx] = r[k];
         v.counts[idx] = 0u;
         if (v.bmove) v.bmove[idx] = 0u;
-#ifndef UPBD_PARITY_BUILD
-        if (v.bfast) v.bfast[idx] = 0u;
-#endif
       }
     }
   }
@@ -214,16 +185,10 @@ __device__ __forceinline__ void b_scatter(const SimView& v, uint32_t vb) {
   v.tmp[v.start[h] + v.ticket[i]] = (uint32_t)i;
 }
 
-#ifndef UPBD_PARITY_BUILD
-// grid-time movement since the list build (upbd_vlist.cuh)
-__device__ __forceinline__ void vl_record_grid(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t h,
-                                               uint32_t slot);
-#endif
-
 // Deterministic membership: particle i goes to start[h] + #{j in bucket : j > i},
 // i.e. descending index inside a bucket, the order Solver._buildGrid's
 // `--cellStart[h]` scatter leaves (src/solver.js:182-183).
-__device__ __forceinline__ void b_rankfix(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
+__device__ __forceinline__ void b_rankfix(const SimView& v, uint32_t vb) {
   const int i = UPBD_VTID;
   if (i >= v.N) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
@@ -241,9 +206,6 @@ __device__ __forceinline__ void b_rankfix(const SimView& v, const DevParams* __r
     v.spos[s + rank] = v.pos[i];
     v.fend[h] = e - solids;  // every member writes the same value
   }
-#ifndef UPBD_PARITY_BUILD
-  if (v.pfl && i >= v.S && P->use_lists && v.scratch[SCR_REBUILD] == 0u) vl_record_grid(v, P, i, h, s + rank);
-#endif
 }
 
 // ------------------------------------------------------------------ fluid
@@ -261,12 +223,6 @@ __device__ __forceinline__ void slot_group(const SimView& v, uint32_t t, uint32_
   i = (e0 < nact) ? v.entries[e0] : 0u;
   fluid = e0 < nact && i >= (uint32_t)v.S;
 }
-
-}  // namespace upbd
-#ifndef UPBD_PARITY_BUILD
-#include "upbd_vlist.cuh"
-#endif
-namespace upbd {
 
 // fluidDensity, src/gpu/wgsl.js:254-279. Every grid entry is active (the
 // grid is built from the active particles of this substep, before bounds).
@@ -862,9 +818,7 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
     return;
   }
   float cx = 0.f, cy = 0.f, cz = 0.f, cnt = 0.f;
-  // a fluid particle's displaced position is its slot copy sfp (the
-  // displacement pass of the product build leaves pos[i] to the bounds pass)
-  const float4 pi = walk ? (iSolid ? v.pos[i] : v.sfp[v.slot[i]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 pi = walk ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
   const float wi = pi.w;
@@ -963,8 +917,8 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   if (!(f & F_ACTIVE)) return;
   const bool iSolid = i < v.S;
   const float r = iSolid ? P->solid_radius : P->fluid_radius;
+  float4 p = v.pos[i];
   const uint32_t sl = v.slot[i];
-  float4 p = iSolid ? v.pos[i] : v.sfp[sl];  // a fluid particle's displaced position is its slot copy
   const float4 o = iSolid ? p : v.spos[sl];  // a fluid particle's density-pass position, read before any store
   // applyDeltaAll
   {
@@ -979,9 +933,7 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   }
   if (stage < 2) {
     v.pos[i] = p;
-#ifdef UPBD_PARITY_BUILD
     if (!iSolid) record_move(v, P, i, sl, o, p);
-#endif
     v.spos[sl] = p;
     return;
   }
@@ -1016,24 +968,13 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   }
   p.x = px; p.y = py; p.z = pz;
   v.pos[i] = p;
-#ifdef UPBD_PARITY_BUILD
   if (!iSolid) record_move(v, P, i, sl, o, p);
-  const float moved = 0.f;
-#else
-  const uint32_t erk = (!iSolid && P->use_lists) ? v.erank[i] : NO_RANK;
-  const float moved = (erk != NO_RANK && vl_record(v, P, i, erk, o, p, culled)) ? 1.f : 0.f;
-  if (culled) atomicOr(&v.scratch[SCR_DIRTY], 1u);  // the next substep rebuilds the lists
-#endif
   v.spos[sl] = p;
   if (stage < 3) return;
   if (culled) {
     // xsph still reads a culled neighbour's velocity (src/gpu/wgsl.js:761
     // does not test its flag): its slot keeps the unchanged velocity
-    const float4 vv = v.vel[i];
-    v.svel[sl] = vv;
-#ifndef UPBD_PARITY_BUILD
-    if (!iSolid && erk != NO_RANK) v.evel[erk] = make_float4(vv.x, vv.y, vv.z, moved);
-#endif
+    v.svel[sl] = v.vel[i];
     return;
   }
   // velocityUpdate
@@ -1053,12 +994,6 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   const float4 nv = make_float4(vx, vy, vz, vw);
   v.vel[i] = nv;
   v.svel[sl] = nv;
-#ifndef UPBD_PARITY_BUILD
-  // w: changed cell after the grid build (xsph's list rule)
-  if (!iSolid && erk != NO_RANK) v.evel[erk] = make_float4(vx, vy, vz, moved);
-#else
-  (void)moved;
-#endif
 }
 
 // solidVisc, src/gpu/wgsl.js:717-735

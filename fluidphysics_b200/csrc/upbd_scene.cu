@@ -194,15 +194,6 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.sfp = cv.take<float4>(v.N);
   L.smove = cv.take<float>(v.N);
   L.bmove = cv.take<uint32_t>(v.T);
-  L.ep = cv.take<uint32_t>(v.N);
-  L.erank = cv.take<uint32_t>(v.N);
-  L.erec = cv.take<uint4>(v.N);
-  L.xlist = cv.take<float4>(v.N);
-  L.epos = cv.take<float4>(v.N);
-  L.edens = cv.take<float2>(v.N);
-  L.evel = cv.take<float4>(v.N);
-  L.pfl = cv.take<uint32_t>(v.N);
-  L.bfast = cv.take<uint32_t>(v.T);
   L.scr = cv.take<uint32_t>(SCR_WORDS);
   L.par = cv.take<DevParams>(1);
   L.bytes = cv.off;
@@ -244,15 +235,6 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.sfp = (float4*)(base + L.sfp);
   v.smove = (float*)(base + L.smove);
   v.bmove = (uint32_t*)(base + L.bmove);
-  v.ep = (uint32_t*)(base + L.ep);
-  v.erank = (uint32_t*)(base + L.erank);
-  v.erec = (uint4*)(base + L.erec);
-  v.xlist = (float4*)(base + L.xlist);
-  v.epos = (float4*)(base + L.epos);
-  v.edens = (float2*)(base + L.edens);
-  v.evel = (float4*)(base + L.evel);
-  v.pfl = (uint32_t*)(base + L.pfl);
-  v.bfast = (uint32_t*)(base + L.bfast);
   v.scratch = (uint32_t*)(base + L.scr);
   if (params) *params = (DevParams*)(base + L.par);
 }
@@ -370,8 +352,6 @@ cudaError_t upload_prepared(const PreparedScene& ps, const SimView& v, cudaStrea
     std::vector<uint32_t> f((size_t)S + ps.n_fluid, F_ACTIVE);
     e = up(v.flags, f.data(), f.size() * 4);
   }
-  // the first substep builds the fluid neighbour lists (product build)
-  if (e == cudaSuccess) e = cudaMemsetAsync(v.scratch + SCR_DIRTY, 0xff, sizeof(uint32_t), st);
   return e;
 }
 
@@ -429,10 +409,6 @@ void fill_dev_params(const upbd_params& p, const upbd_scene_desc& desc, DevParam
   // exact (the marked set only grows by the 1e-5 slack of mark_fluid_near)
   const double rsum = (double)(d.solid_radius + d.fluid_radius);
   d.use_mark = (rsum * 1.0001 < p.cell_size * (1.0 - 1e-6)) ? 1 : 0;
-  // neighbour lists kept across substeps (product build) need every pair
-  // within H in adjacent cells: H at most the cell size (deriveOpts makes
-  // them equal; the float H may exceed the double cell size by its rounding)
-  d.use_lists = ((double)d.fluid_h <= p.cell_size * (1.0 + 1e-6)) ? 1 : 0;
 }
 
 }  // namespace upbd

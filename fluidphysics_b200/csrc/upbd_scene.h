@@ -34,7 +34,7 @@ void build_scene(const upbd_scene_desc& d, HostScene& out);
 struct SceneLayout {
   size_t pos, prev, vel, delta, dens, flags, cons, adj, counts, start, entries, tmp, ticket, cell, tiles;
   size_t tidx, tvol, tadj, mark, spos, sdens, svel, slot, fend, nbr, ncount, aoth, ascl, ccount, clist;
-  size_t sbuf, sfp, smove, bmove, ep, erank, erec, xlist, epos, edens, evel, pfl, bfast, scr, par;
+  size_t sbuf, sfp, smove, bmove, scr, par;
   size_t bytes;
 };
 

@@ -234,14 +234,6 @@ class Sim:
         self._ck(self.lib.upbd_groups(self.h, g.ctypes.data_as(C.POINTER(C.c_int32))))
         return g
 
-    def list_stats(self) -> dict:
-        """Neighbour-list statistics of the product build's fluid gathers
-        (rebuilds, walkers, listed, complete, max_len, mean_len); zeros in the
-        parity build."""
-        li = L.ListInfo()
-        self._ck(self.lib.upbd_list_stats(self.h, C.byref(li)))
-        return {f: getattr(li, f) for f, _ in L.ListInfo._fields_}
-
 
 def sim_from_scene(scene: S.Scene, variant: str = "product") -> Sim:
     """Create a Sim for a Scene and load its initial fluid block."""

@@ -366,25 +366,6 @@ int upbd_grid_build_noalloc(const void* pos4, const void* flags, int32_t n, int3
                             double cell_size, void* counts, void* offsets, void* entries,
                             void* stream);
 
-/* Neighbour-list statistics of the fluid gathers. The product build keeps
- * each fluid particle's neighbour list across substeps and rebuilds the
- * lists only when particles moved too far or the state changed from outside;
- * the parity build walks the hash buckets every substep and reports zeros.
- * (No counterpart in the reference, which walks the buckets every substep.) */
-typedef struct upbd_list_info {
-  uint64_t rebuilds;  /* substeps since creation whose density pass rebuilt every list */
-  uint32_t walkers;   /* fluid particles whose density or xsph pass walked the buckets in
-                         the last substep for want of a usable list (those whose 27
-                         buckets share a bucket always walk and are not counted) */
-  uint32_t listed;    /* active fluid particles whose last density pass read its list */
-  uint32_t complete;  /* active fluid particles holding a complete list */
-  uint32_t max_len;   /* entries of the longest list */
-  double mean_len;    /* mean list length over the active fluid */
-} upbd_list_info;
-
-/* Fills *out; waits for the handle's stream. */
-int upbd_list_stats(upbd_sim* sim, upbd_list_info* out);
-
 /* Kernels this handle has launched so far (each replay of a captured frame
  * counts its kernel nodes). Instrumentation for benchmarks. */
 uint64_t upbd_launch_count(upbd_sim* sim);

@@ -106,11 +106,10 @@ def test_launches_per_frame_do_not_depend_on_scene_count():
             l0 = b.launches
             step(b, 3)
             counts.append((b.launches - l0) / 3)
-    # 5 substeps x (integrate, scan, scatter, rankfix, the density rebuild
-    # (returns at once on substeps that keep their lists), density, disp,
+    # 5 substeps x (integrate, scan, scatter, rankfix, density, disp,
     # 3 x solve-and-apply, bonds+contacts, apply+bounds+velocity, xsph with
     # its apply) + the active count
-    assert counts[0] == counts[1] == 5 * 13 + 1
+    assert counts[0] == counts[1] == 5 * 12 + 1
 
 
 def test_capacity_and_budget_are_enforced():
