@@ -171,6 +171,7 @@ _SIGS = [
     ("upbd_write_tets", C.c_int, [_P, _U]),
     ("upbd_set_fluid_next", C.c_int, [_P, C.c_int32]),
     ("upbd_groups", C.c_int, [_P, C.POINTER(C.c_int32)]),
+    ("upbd_groups_device", C.c_int, [_P, C.c_void_p]),
     ("upbd_grid_build", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
     ("upbd_grid_build_noalloc", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
     ("upbd_launch_count", C.c_uint64, [_P]),

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/upbd.h"
+#include "upbd_groups.cuh"
 #include "upbd_kernels.cuh"
 #include "upbd_kinds.h"
 #include "upbd_scene.h"
@@ -1114,28 +1115,39 @@ int upbd_set_fluid_next(upbd_sim* s, int32_t next) {
 // Solver._recomputeGroups, src/solver.js:488-499 — union-find with path
 // halving over alive constraints in constraint order, on the host over the
 // downloaded alive flags (the same sequential algorithm, so root ids match).
-int upbd_groups(upbd_sim* s, int32_t* group) {
-  if (!s || !group) return UPBD_ERR_INVALID;
-  cudaSetDevice(s->device);
+int upbd_groups_device(upbd_sim* s, int32_t* d_group) {
+  if (!s) return UPBD_ERR_INVALID;
   const int S = s->v.S, C = s->v.C;
-  std::vector<uint4> cons(C);
-  if (C > 0) UPBD_CK(s, cudaMemcpyAsync(cons.data(), s->v.cons, (size_t)C * 16, cudaMemcpyDeviceToHost, s->stream));
-  UPBD_CK(s, cudaStreamSynchronize(s->stream));
-  std::vector<int32_t> parent(S);
-  std::iota(parent.begin(), parent.end(), 0);
-  auto find = [&parent](int x) {
-    while (parent[x] != x) {
-      parent[x] = parent[parent[x]];
-      x = parent[x];
-    }
-    return x;
-  };
-  for (int c = 0; c < C; c++) {
-    if (!cons[c].w) continue;
-    const int ra = find((int)cons[c].x), rb = find((int)cons[c].y);
-    if (ra != rb) parent[ra] = rb;
+  if (S == 0) return UPBD_OK;
+  if (!d_group) return UPBD_ERR_INVALID;
+  cudaSetDevice(s->device);
+  cudaStream_t st = s->stream;
+  int32_t* par = reinterpret_cast<int32_t*>(s->v.tmp);  // the grid's scatter buffer, N >= S words
+  if (S <= GROUPS_SMEM_MAX) {
+    const size_t smem = (size_t)S * sizeof(int32_t);
+    if (smem > 48 * 1024)
+      UPBD_CK(s, cudaFuncSetAttribute(k_groups_replay<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    k_groups_replay<true><<<1, 32, smem, st>>>(s->v.cons, C, S, par);
+  } else {
+    k_groups_replay<false><<<1, 32, 0, st>>>(s->v.cons, C, S, par);
   }
-  for (int i = 0; i < S; i++) group[i] = find(i);
+  UPBD_KCK(s);
+  k_groups_label<<<blocks_for(S), 256, 0, st>>>(par, S, d_group);
+  UPBD_KCK(s);
+  return UPBD_OK;
+}
+
+int upbd_groups(upbd_sim* s, int32_t* group) {
+  if (!s || (!group && s->v.S > 0)) return UPBD_ERR_INVALID;
+  const int S = s->v.S;
+  if (S == 0) return UPBD_OK;
+  // labels land in the grid's ticket buffer (N >= S words, free between
+  // substeps) and come back in one copy
+  int32_t* d = reinterpret_cast<int32_t*>(s->v.ticket);
+  if (int rc = upbd_groups_device(s, d)) return rc;
+  UPBD_CK(s, cudaMemcpyAsync(group, d, (size_t)S * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+  UPBD_CK(s, cudaStreamSynchronize(s->stream));
   return UPBD_OK;
 }
 

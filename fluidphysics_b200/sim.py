@@ -230,9 +230,16 @@ class Sim:
         self._ck(self.lib.upbd_set_fluid_next(self.h, int(k)))
 
     def groups(self) -> np.ndarray:
+        """Solver._recomputeGroups (src/solver.js:488-499): the root label of
+        every solid after the union-find over the alive constraints."""
         g = np.empty(self.info.solid_n, np.int32)
         self._ck(self.lib.upbd_groups(self.h, g.ctypes.data_as(C.POINTER(C.c_int32))))
         return g
+
+    def groups_device(self, out_ptr: int) -> None:
+        """The same labels into device memory (solid_n int32 at out_ptr), on
+        the simulation's stream, with no host synchronisation."""
+        self._ck(self.lib.upbd_groups_device(self.h, C.c_void_p(out_ptr)))
 
 
 def sim_from_scene(scene: S.Scene, variant: str = "product") -> Sim:

@@ -306,8 +306,14 @@ int upbd_write_tets(upbd_sim* sim, const uint32_t* tets5);
  * hose ring buffer, 0 <= next < max_fluid. */
 int upbd_set_fluid_next(upbd_sim* sim, int32_t next);
 /* Solver._recomputeGroups — src/solver.js:488-499: union-find over alive
- * constraints; group[solid_n] = root id. */
+ * constraints in index order; group[solid_n] = the root id the reference's
+ * sequence of unions leaves (bit for bit). Computed on the GPU
+ * (upbd_groups_device) and copied back; returns after the copy. */
 int upbd_groups(upbd_sim* sim, int32_t* group);
+/* The same labels written to device memory d_group[solid_n] on the sim's
+ * stream, without a host synchronisation (capturable in a CUDA graph).
+ * Uses the grid build's scratch, which is free between substeps. */
+int upbd_groups_device(upbd_sim* sim, int32_t* d_group);
 
 /* Pass ids for upbd_substep_partial (order of src/gpu/sim.js:354-385). */
 #define UPBD_PASS_INTEGRATE      1

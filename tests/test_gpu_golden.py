@@ -57,9 +57,9 @@ def test_grid_and_cut_of_default_scene_match_solver_js():
     assert digest(sim.read_constraints()[:, 3].astype(np.uint8)) == case["digest"]["consAlive"]
 
 
-def test_pick_rays_match_solver_js():
-    """pickSolid rays of the golden case, on the same body positions."""
-    case = J["cases"]["c1_tools"]
+def _c1_tools_sim():
+    """A GPU sim of the CPU scene whose body holds the positions the golden
+    tool case ran on (the settled substep's output)."""
     sc = S.cpu_scene()
     sim = sim_from_scene(sc)
     # the golden picks ran on the settled-substep output; rebuild that body state
@@ -75,9 +75,31 @@ def test_pick_rays_match_solver_js():
     st = sim.read_state()
     st["pos"][:, :3] = o.get("pos").reshape(-1, 3)
     sim.write_state(pos=st["pos"])
+    return sim
+
+
+def test_pick_rays_match_solver_js():
+    """pickSolid rays of the golden case, on the same body positions."""
+    case = J["cases"]["c1_tools"]
+    sim = _c1_tools_sim()
     for p in case["picks"]:
         i, t = sim.pick(p["o"], p["d"], p["maxPerp"])
         if p["id"] is None:
             assert i == -1
         else:
             assert i == p["id"] and t == p["t"]
+
+
+def test_groups_after_cuts_match_solver_js():
+    """Solver._recomputeGroups (src/solver.js:488-499) on the GPU after the
+    golden case's cuts: the alive flags and every solid's group label equal
+    those the unmodified solver.js produced (labels are the roots its
+    order of unions leaves, not component minima)."""
+    case = J["cases"]["c1_tools"]
+    sim = _c1_tools_sim()
+    for c in case["cuts"]:
+        assert sim.slice_now(c["o"], c["d1"], c["d2"]) == c["count"]
+        assert digest(sim.read_constraints()[:, 3].astype(np.uint8)) == c["alive"]
+    g = sim.groups()
+    assert g.tolist() == case["group"]
+    assert len(set(case["group"])) > 1
