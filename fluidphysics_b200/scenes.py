@@ -87,6 +87,21 @@ GPU_DEFAULTS = {
 }
 
 
+def merge_gpu_opts(opts: dict) -> dict:
+    """The options object of the GpuSim constructor (src/gpu/sim.js:78-84):
+    DEFAULTS overlaid with opts, params merged the same way, and SOLID_DIM2
+    resolved (opts' value, else the companion cube's edge (SOLID_DIM - 1) /
+    cbrt(20), rounded, + 1, at least 2) — what a snapshot's `opts` holds,
+    with the keys in the reference's order."""
+    o = {**GPU_DEFAULTS, **{k: v for k, v in opts.items() if k != "params"}}
+    o["params"] = {**GPU_DEFAULTS["params"], **opts.get("params", {})}
+    dim2 = o.get("SOLID_DIM2")
+    if dim2 is None:
+        dim2 = max(2, js_round((o["SOLID_DIM"] - 1) / 20 ** (1 / 3)) + 1)
+    o["SOLID_DIM2"] = int(dim2)
+    return o
+
+
 def default_desc() -> L.SceneDesc:
     d = L.SceneDesc()
     _fill_default_desc(d)

@@ -267,10 +267,7 @@ class GpuSim:
         self.sim = Sim(self.desc, self.params, variant)
         # the merged options of the constructor (src/gpu/sim.js:78-84), with
         # the companion cube's size resolved: what a snapshot carries
-        o = {**S.GPU_DEFAULTS, **{k: v for k, v in opts.items() if k != "params"}}
-        o["params"] = {**S.GPU_DEFAULTS["params"], **opts.get("params", {})}
-        o["SOLID_DIM2"] = int(self.desc.solid_dim2)
-        self.o = o
+        self.o = S.merge_gpu_opts(opts)
         i = self.sim.info
         self.SOLID_N, self.N1, self.TOTAL = i.solid_n, i.n1, i.total
         self.DIM2, self.NUM_CONS, self.NUM_TETS = i.dim2, i.num_cons, i.num_tets

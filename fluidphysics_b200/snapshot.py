@@ -37,27 +37,75 @@ def _unb64(s: str, dtype, cols: int | None = None) -> np.ndarray:
     return a.reshape(-1, cols) if cols else a
 
 
-def snapshot(gs: GpuSim) -> dict:
-    """The full particle state of a GpuSim as the reference's snapshot."""
-    st = gs.sim.read_state()
-    cons = gs.sim.read_constraints()
-    tets = gs.sim.read_tets()
+def js_numbers(v):
+    """A JSON-able value with every integral float as an int: JavaScript
+    numbers have one type, and JSON.stringify prints 3.0 as 3."""
+    if isinstance(v, dict):
+        return {k: js_numbers(x) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [js_numbers(x) for x in v]
+    if isinstance(v, float) and v.is_integer() and abs(v) < 2.0 ** 53:
+        return int(v)
+    return v
+
+
+def snapshot_from_arrays(opts: dict, fluid_next: int, num_cons: int, state: dict, cons: np.ndarray,
+                         tets: np.ndarray) -> dict:
+    """The snapshot object of GpuSim.snapshot (src/gpu/sim.js:493-513) for
+    host arrays: the same keys in the same order, each buffer the base64
+    (b64encode, src/gpu/sim.js:3-9) of its raw little-endian bytes."""
     return {
         "version": 1,
         "app": "slice-splash-gpu",
-        "opts": json.loads(json.dumps(gs.o)),
-        "fluidNext": int(gs.fluidNext),
-        "numCons": int(gs.NUM_CONS),
+        "opts": js_numbers(json.loads(json.dumps(opts))),
+        "fluidNext": int(fluid_next),
+        "numCons": int(num_cons),
         "buffers": {
-            "pos": _b64(st["pos"].astype("<f4")),
-            "prev": _b64(st["prev"].astype("<f4")),
-            "vel": _b64(st["vel"].astype("<f4")),
-            "flags": _b64(st["flags"].astype("<u4")),
-            "density": _b64(st["density"].astype("<f4")),
-            "cons": _b64(cons.astype("<u4")),
-            "tets": _b64(tets.astype("<u4")),
+            "pos": _b64(np.asarray(state["pos"]).astype("<f4")),
+            "prev": _b64(np.asarray(state["prev"]).astype("<f4")),
+            "vel": _b64(np.asarray(state["vel"]).astype("<f4")),
+            "flags": _b64(np.asarray(state["flags"]).astype("<u4")),
+            "density": _b64(np.asarray(state["density"]).astype("<f4")),
+            "cons": _b64(np.asarray(cons).astype("<u4")),
+            "tets": _b64(np.asarray(tets).astype("<u4")),
         },
     }
+
+
+def snapshot(gs: GpuSim) -> dict:
+    """The full particle state of a GpuSim as the reference's snapshot."""
+    return snapshot_from_arrays(gs.o, gs.fluidNext, gs.NUM_CONS, gs.sim.read_state(),
+                                gs.sim.read_constraints(), gs.sim.read_tets())
+
+
+def decode_buffers(snap: dict, total: int, num_tets: int, keep_grabs: bool = False) -> dict:
+    """The arrays GpuSim.restore (src/gpu/sim.js:515-545) writes from a
+    snapshot of a scene with `total` particles and `num_tets` tets: pos,
+    prev, vel, density, flags (grab bits cleared unless keep_grabs), cons,
+    and tets when the snapshot holds exactly num_tets of them (older files
+    have none, and keep the scene's own). Missing buffers are left out."""
+    b = snap["buffers"]
+    out = {}
+    for name, cols in (("pos", 4), ("prev", 4), ("vel", 4), ("density", 2)):
+        if name in b:
+            a = _unb64(b[name], np.float32, cols)
+            if a.shape[0] != total:
+                raise ValueError(f"snapshot {name} holds {a.shape[0]} particles, the scene {total}")
+            out[name] = a
+    if "flags" in b:
+        f = _unb64(b["flags"], np.uint32)
+        if f.shape[0] != total:
+            raise ValueError(f"snapshot flags hold {f.shape[0]} particles, the scene {total}")
+        if not keep_grabs:
+            f = f & np.uint32(~L.F_GRABBED & 0xFFFFFFFF)
+        out["flags"] = f
+    if "cons" in b:
+        out["cons"] = _unb64(b["cons"], np.uint32, 4)
+    if "tets" in b:
+        t = _unb64(b["tets"], np.uint32)
+        if num_tets and t.size == num_tets * 5:
+            out["tets"] = t.reshape(-1, 5)
+    return out
 
 
 def restore(gs: GpuSim, snap: dict, keep_grabs: bool = False) -> None:
@@ -65,27 +113,13 @@ def restore(gs: GpuSim, snap: dict, keep_grabs: bool = False) -> None:
     Standalone snapshots drop the grab bits (no release will come); a
     recording keeps them, since the grab targets live in the buffers. A
     snapshot without tets (older files) leaves the tets as they are."""
-    b = snap["buffers"]
-    n = gs.TOTAL
-    kw = {}
-    for name, cols in (("pos", 4), ("prev", 4), ("vel", 4), ("density", 2)):
-        if name in b:
-            a = _unb64(b[name], np.float32, cols)
-            if a.shape[0] != n:
-                raise ValueError(f"snapshot {name} holds {a.shape[0]} particles, the scene {n}")
-            kw[name] = a
-    if "flags" in b:
-        f = _unb64(b["flags"], np.uint32)
-        if not keep_grabs:
-            f = f & np.uint32(~L.F_GRABBED & 0xFFFFFFFF)
-        kw["flags"] = f
+    a = decode_buffers(snap, gs.TOTAL, gs.NUM_TETS, keep_grabs)
+    kw = {k: a[k] for k in ("pos", "prev", "vel", "density", "flags") if k in a}
     gs.sim.write_state(**kw)
-    if "cons" in b:
-        gs.sim.write_constraints(_unb64(b["cons"], np.uint32, 4))
-    if "tets" in b:
-        t = _unb64(b["tets"], np.uint32)
-        if t.size == gs.NUM_TETS * 5 and gs.NUM_TETS:
-            gs.sim.write_tets(t.reshape(-1, 5))
+    if "cons" in a:
+        gs.sim.write_constraints(a["cons"])
+    if "tets" in a:
+        gs.sim.write_tets(a["tets"])
     gs.sim.set_fluid_next(int(snap.get("fluidNext", 0)))
 
 

@@ -77,3 +77,33 @@ def test_recording_replays_exactly():
         a.encode()
     b = SN.replay(SN.loads(SN.dumps(bundle)), tail_frames=tail)
     same(a, b, "replay")
+
+
+def test_reference_written_snapshot_loads_exactly():
+    """A snapshot that the reference's own GpuSim.snapshot wrote
+    (tests/golden/app_js.json, made by tests/golden/make_golden_app.py from
+    seeded buffers) loads into a GpuSim built from its options: every buffer
+    lands bit for bit (grab bits dropped, as a standalone restore does), and
+    snapshotting the loaded scene writes the same object back."""
+    import json
+    from pathlib import Path
+    gold = Path(__file__).resolve().parent / "golden"
+    case = json.loads((gold / "app_js.json").read_text())["cases"]["snapshot"]
+    npz = np.load(gold / "app_js.npz")
+    snap = case["snapshot"]
+    gs = SN.load_snapshot(snap)
+    assert (gs.TOTAL, gs.NUM_CONS, gs.NUM_TETS) == (case["total"], case["num_cons"], case["num_tets"])
+    st = gs.sim.read_state()
+    for k in ("pos", "prev", "vel", "density"):
+        assert st[k].tobytes() == npz[k].tobytes(), k
+    assert np.array_equal(st["flags"], npz["flags"] & np.uint32(0xFFFFFFFD))
+    assert np.array_equal(gs.sim.read_constraints(), npz["cons"])
+    assert np.array_equal(gs.sim.read_tets(), npz["tets"])
+    assert gs.fluidNext == snap["fluidNext"]
+    back = SN.snapshot(gs)
+    want = dict(snap)
+    want["buffers"] = dict(snap["buffers"])
+    want["buffers"]["flags"] = SN.snapshot_from_arrays(
+        {}, 0, 0, {**{k: npz[k] for k in ("pos", "prev", "vel", "density")},
+                   "flags": npz["flags"] & np.uint32(0xFFFFFFFD)}, npz["cons"], npz["tets"])["buffers"]["flags"]
+    assert json.dumps(back) == json.dumps(want)
