@@ -708,6 +708,13 @@ def main() -> None:
     step_gbs = B_sub * sc.substeps * K / (ms / 1e3) / 1e9
     roofline["step_achieved_gbs"] = step_gbs
     roofline["step_frac"] = step_gbs / hbm
+    # launch floor: the same frame graph with every kernel emptied (same nodes,
+    # grids, dependencies and side-stream branches), replayed back to back
+    floor_ms, floor_nodes = sim.graph_floor(sc.dt, sc.substeps, 200)
+    launch_floor = {"empty_graph_ms": floor_ms, "kernel_nodes": floor_nodes,
+                    "share_of_frame": floor_ms / (t_max / K),
+                    "how": "the captured frame graph with each kernel node's kernel replaced by an empty one "
+                           "of the same grid and block, 200 replays timed by CUDA events"}
 
     sim.close()
     large = run_large(args, stream) if args.large_frames > 0 else None
@@ -747,6 +754,7 @@ def main() -> None:
                             "frame (device staging copy, host copy overlapping the next frame), "
                             "upbd_read_wait before the clock stops"},
             "roofline": roofline,
+            "launch_floor": launch_floor,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clk,

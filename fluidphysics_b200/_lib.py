@@ -176,6 +176,7 @@ _SIGS = [
     ("upbd_grid_build_noalloc", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, _P, _P, _P]),
     ("upbd_launch_count", C.c_uint64, [_P]),
     ("upbd_profile_frame", C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(C.c_double), _U]),
+    ("upbd_profile_graph_floor", C.c_int, [_P, C.c_double, C.c_int32, C.c_int32, C.POINTER(C.c_double), _U]),
     ("upbd_kernel_name", C.c_char_p, [C.c_int32]),
     # scene batch (include/upbd_batch.h)
     ("upbd_batch_default_desc", C.c_int, [C.POINTER(BatchDesc)]),

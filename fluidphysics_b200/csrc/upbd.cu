@@ -1265,6 +1265,73 @@ int upbd_profile_frame(upbd_sim* s, double dt, int32_t substeps, double* ms, uin
   return UPBD_OK;
 }
 
+// The launch floor of a frame graph: the frame is captured as upbd_step
+// captures it, then every kernel node of a copy is given an empty kernel with
+// the node's own grid and block, so the copy keeps the graph's shape (nodes,
+// dependencies, the side-stream branches, the memset nodes) and does no work.
+// Its replay time is what the frame pays for launching and ordering its
+// kernels. Nothing in the simulation's state changes.
+int upbd_profile_graph_floor(upbd_sim* s, double dt, int32_t substeps, int32_t reps, double* floor_ms,
+                             uint32_t* kernel_nodes) {
+  if (!s || !floor_ms || !kernel_nodes || substeps < 1 || substeps > 1000 || reps < 1) return UPBD_ERR_INVALID;
+  cudaSetDevice(s->device);
+  cudaGraph_t g = nullptr;
+  UPBD_CK(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  const uint64_t before = s->launches;
+  int rc = launch_frame(s, substeps, 0u, false);
+  cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+  s->launches = before;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (ce != cudaSuccess) return fail(s, UPBD_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+  size_t n = 0;
+  cudaGraphGetNodes(g, nullptr, &n);
+  std::vector<cudaGraphNode_t> nodes(n);
+  cudaGraphGetNodes(g, nodes.data(), &n);
+  uint32_t nk = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+    cudaKernelNodeParams kp;
+    ce = cudaGraphKernelNodeGetParams(nd, &kp);
+    if (ce == cudaSuccess) {
+      kp.func = (void*)k_empty;
+      kp.sharedMemBytes = 0;
+      kp.kernelParams = nullptr;
+      kp.extra = nullptr;
+      ce = cudaGraphKernelNodeSetParams(nd, &kp);
+    }
+    if (ce != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return fail(s, UPBD_ERR_CUDA, std::string("kernel node: ") + cudaGetErrorString(ce));
+    }
+    nk++;
+  }
+  cudaGraphExec_t ge;
+  ce = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail(s, UPBD_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  for (int k = 0; k < 3; k++) cudaGraphLaunch(ge, s->stream);
+  cudaEventRecord(a, s->stream);
+  for (int k = 0; k < reps; k++) cudaGraphLaunch(ge, s->stream);
+  cudaEventRecord(b, s->stream);
+  ce = cudaEventSynchronize(b);
+  float t = 0.f;
+  if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaGraphExecDestroy(ge);
+  if (ce != cudaSuccess) return fail(s, UPBD_ERR_CUDA, std::string("floor timing: ") + cudaGetErrorString(ce));
+  *floor_ms = (double)t / reps;
+  *kernel_nodes = nk;
+  return UPBD_OK;
+}
+
 }  // extern "C"
 
 // ===================================================== allocation-free grid build

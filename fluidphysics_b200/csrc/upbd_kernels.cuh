@@ -269,6 +269,9 @@ __global__ void k_grab_release(SimView v) {
 }
 
 // GpuSim.clearFluid, src/gpu/sim.js:294-297
+// the body of every kernel node in upbd_profile_graph_floor's copy of a frame
+__global__ void k_empty() {}
+
 __global__ void k_drain(SimView v) {
   const int i = v.S + (int)UPBD_TID;
   if (i < v.N) v.flags[i] = 0u;

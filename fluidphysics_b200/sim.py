@@ -82,6 +82,16 @@ class Sim:
     def launches(self) -> int:
         return int(self.lib.upbd_launch_count(self.h))
 
+    def graph_floor(self, dt: float, substeps: int, reps: int = 200) -> tuple[float, int]:
+        """(ms per replay, kernel nodes) of the frame graph with every kernel
+        replaced by an empty one of the same grid: the frame's launch floor."""
+        import ctypes as C
+        ms = C.c_double()
+        nk = C.c_uint32()
+        self._ck(self.lib.upbd_profile_graph_floor(self.h, float(dt), int(substeps), int(reps), C.byref(ms),
+                                                   C.byref(nk)))
+        return float(ms.value), int(nk.value)
+
     # ------------------------------------------------------------ stepping
     def step(self, dt: float, substeps: int) -> None:
         self._ck(self.lib.upbd_step(self.h, float(dt), int(substeps)))

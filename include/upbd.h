@@ -385,6 +385,17 @@ uint64_t upbd_launch_count(upbd_sim* sim);
 int upbd_profile_frame(upbd_sim* sim, double dt, int32_t substeps, double* ms, uint32_t* launches);
 const char* upbd_kernel_name(int32_t kind);
 
+/* Launch floor of the frame graph: captures one frame of `substeps` substeps
+ * the way upbd_step does, replaces every kernel node's kernel by an empty one
+ * with the node's own grid and block (the graph's nodes and dependencies are
+ * kept), and times `reps` replays of that copy with CUDA events on the
+ * simulation's stream. *floor_ms = device time per replay, *kernel_nodes =
+ * kernel nodes in the frame. The simulation's state is not touched.
+ * Synchronous. Instrumentation for benchmarks; no counterpart in the
+ * reference (WebGPU gives no such measurement). */
+int upbd_profile_graph_floor(upbd_sim* sim, double dt, int32_t substeps, int32_t reps, double* floor_ms,
+                             uint32_t* kernel_nodes);
+
 #ifdef __cplusplus
 }
 #endif
