@@ -307,23 +307,25 @@ def run_batched(args, stream, hbm: float) -> dict:
               for k in np.argsort(-msk) if ln[k]}
     info = b.info()
     b.close()
-    # plain per-scene path on every 8th scene
+    # plain per-scene path on every 8th scene, over the same frames the batch
+    # was timed on: 6 untimed frames (the batch's warm-up and tuning frames
+    # leave it 6 frames in), then K timed graph frames
     sample = scs[::8]
     pp_units, pp_ms = 0.0, 0.0
     for sc in sample:
         sim = sim_from_scene(sc)
         sim.set_stream(stream.cuda_stream)
-        for _ in range(3):
+        for _ in range(6):
             sim.step(dt, nsub)
         sim.sync()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(stream)
-        for _ in range(20):
+        for _ in range(K):
             sim.step(dt, nsub)
         a1.record(stream)
         sim.sync()
         pp_ms += a0.elapsed_time(a1)
-        pp_units += (sc.solid_n + sim.active_count()) * nsub * 20
+        pp_units += (sc.solid_n + sim.active_count()) * nsub * K  # counted as the batched value counts
         sim.close()
     pp = pp_units / (pp_ms / 1e3)
     return {
@@ -340,7 +342,7 @@ def run_batched(args, stream, hbm: float) -> dict:
         "step_achieved_gbs": step_gbs, "step_frac": step_gbs / hbm,
         "plain_per_scene": {"value": pp, "unit": UNIT,
                             "sample": f"{len(sample)} of the scenes (every 8th), each its own single-scene "
-                                      "handle, 20 graph frames after 3 warm-up frames"},
+                                      f"handle, graph frames 7..{6 + K} (the frames the batch was timed on)"},
         "speedup_vs_plain_per_scene": value / pp,
     }
 
@@ -471,6 +473,30 @@ def run_served(args, batched: dict | None) -> dict:
     return out
 
 
+def batched_capture(scenes: int, frames: int) -> None:
+    """Builds the uneven batch of `scenes` scenes (the batched line's scenes,
+    the compact hash-table rule, 256-thread blocks, 16 CTAs per SM), steps it
+    `frames` frames, then runs one more frame between cudaProfilerStart and
+    cudaProfilerStop: the window of the batched kernel captures."""
+    import torch
+    from fluidphysics_b200 import batch as B
+
+    scs = B.batch_scenes(scenes, table="compact")
+    with B.Batch(max_scenes=max(256, scenes), ctas_per_sm=16) as b:
+        for sc in scs:
+            b.add_scene(sc)
+        for _ in range(frames):
+            b.step(1 / 60, 5)
+        b.sync()
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        b.step(1 / 60, 5)
+        b.sync()
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
+        print(json.dumps({"batched_capture_scenes": scenes, "bytes": int(b.info().bytes_in_use)}))
+
+
 def settled_capture(frames: int) -> None:
     """Steps the default scene `frames` frames, then runs 3 more between
     cudaProfilerStart and cudaProfilerStop: the settled-state window that the
@@ -523,8 +549,14 @@ def main() -> None:
                     help="profiling mode: step the default scene this many frames on its graph (slice "
                          "at frame 60), bracket the next 3 frames with cudaProfilerStart/Stop for "
                          "ncu --profile-from-start off, and exit (no bench line)")
+    ap.add_argument("--batched-capture", type=int, default=0,
+                    help="profiling mode: build a batch of this many of the batched line's scenes, step "
+                         "it 10 frames, bracket the next frame with cudaProfilerStart/Stop, and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.batched_capture > 0:
+        batched_capture(args.batched_capture, 10)
+        return
 
     if args.impl == "reference":
         run_reference(args)

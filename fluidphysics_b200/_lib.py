@@ -223,12 +223,17 @@ class UpbdError(RuntimeError):
         self.code = code
 
 
+LIB_NAMES = {"product": "libupbd.so", "parity": "libupbd_parity.so", "fp64": "libupbd_fp64.so"}
+
+
 def lib_path(variant: str = "product") -> Path:
-    return HERE / ("libupbd.so" if variant == "product" else "libupbd_parity.so")
+    return HERE / LIB_NAMES[variant]
 
 
 def load(variant: str = "product") -> C.CDLL:
-    """Load libupbd.so ("product") or libupbd_parity.so ("parity")."""
+    """Load libupbd.so ("product"), libupbd_parity.so ("parity") or the
+    test-only libupbd_fp64.so ("fp64": the same pass bodies on double, the
+    single-scene entry points only)."""
     if variant in _libs:
         return _libs[variant]
     path = lib_path(variant)
@@ -238,6 +243,8 @@ def load(variant: str = "product") -> C.CDLL:
             "(there is no non-CUDA fallback)")
     lib = C.CDLL(str(path))
     for name, res, args in _SIGS:
+        if variant == "fp64" and name.startswith(("upbd_batch_", "upbd_server_")):
+            continue  # the FP64 build holds the single-scene library only
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args

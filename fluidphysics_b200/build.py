@@ -5,6 +5,9 @@ Outputs (next to this file):
   libupbd_parity.so  the same sources with --fmad=false, so every FP32
                      operation rounds exactly as the CPU oracle's does
                      (per-pass bit-exact parity checks)
+  libupbd_fp64.so    test-only: the single-scene library with the pass
+                     bodies instantiated on double (UPBD_FP64_BUILD), the
+                     reference trajectory of the 600-frame drift test
 
 Both are cross-compiled with nvcc; no GPU is needed to build.
 """
@@ -27,6 +30,7 @@ SOURCES = ["upbd.cu", "upbd_scene.cu", "upbd_batch.cu", "upbd_server.cu"]
 TARGETS = {
     "libupbd.so": SOURCES,
     "libupbd_parity.so": SOURCES,
+    "libupbd_fp64.so": ["upbd.cu", "upbd_scene.cu"],
 }
 
 
@@ -60,6 +64,8 @@ def build(force: bool = False, verbose: bool = False) -> list[Path]:
         flags = list(COMMON)
         if name == "libupbd_parity.so":
             flags += ["--fmad=false", "-DUPBD_PARITY_BUILD=1"]
+        if name == "libupbd_fp64.so":
+            flags += ["-DUPBD_FP64_BUILD=1"]
         cmd = [nvcc, *ARCH, *flags, "-o", str(out) + ".tmp", *[str(CSRC / s) for s in srcs]]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

@@ -718,11 +718,11 @@ int upbd_reset_solid(upbd_sim* s) {
   // GpuSim.resetSolid, src/gpu/sim.js:283-292: the whole pos/prev buffers
   // (fluid slots included) back to the initial data, every velocity zeroed,
   // solids' flags and density reset, constraints and tets pristine.
-  UPBD_CK(s, cudaMemcpyAsync(v.pos, s->init_pos.data(), (size_t)v.N * 16, cudaMemcpyHostToDevice, st));
-  UPBD_CK(s, cudaMemcpyAsync(v.prev, s->init_pos.data(), (size_t)v.N * 16, cudaMemcpyHostToDevice, st));
-  UPBD_CK(s, cudaMemsetAsync(v.vel, 0, (size_t)v.N * 16, st));
+  UPBD_CK(s, state_to_device((real*)v.pos, (const float*)s->init_pos.data(), (size_t)v.N, 4, v, st));
+  UPBD_CK(s, state_to_device((real*)v.prev, (const float*)s->init_pos.data(), (size_t)v.N, 4, v, st));
+  UPBD_CK(s, cudaMemsetAsync(v.vel, 0, (size_t)v.N * sizeof(real4), st));
   if (v.S > 0) {
-    UPBD_CK(s, cudaMemsetAsync(v.density, 0, (size_t)v.S * 8, st));
+    UPBD_CK(s, cudaMemsetAsync(v.density, 0, (size_t)v.S * sizeof(real2), st));
     std::vector<uint32_t> f(v.S, F_ACTIVE);
     UPBD_CK(s, cudaMemcpyAsync(v.flags, f.data(), (size_t)v.S * 4, cudaMemcpyHostToDevice, st));
     UPBD_CK(s, cudaStreamSynchronize(st));
@@ -930,10 +930,11 @@ int upbd_read_state(upbd_sim* s, float* pos4, float* prev4, float* vel4, float* 
   cudaSetDevice(s->device);
   const size_t N = (size_t)s->v.N;
   cudaStream_t st = s->stream;
-  if (pos4) UPBD_CK(s, cudaMemcpyAsync(pos4, s->v.pos, N * 16, cudaMemcpyDeviceToHost, st));
-  if (prev4) UPBD_CK(s, cudaMemcpyAsync(prev4, s->v.prev, N * 16, cudaMemcpyDeviceToHost, st));
-  if (vel4) UPBD_CK(s, cudaMemcpyAsync(vel4, s->v.vel, N * 16, cudaMemcpyDeviceToHost, st));
-  if (density2) UPBD_CK(s, cudaMemcpyAsync(density2, s->v.density, N * 8, cudaMemcpyDeviceToHost, st));
+  const SimView& v = s->v;
+  if (pos4) UPBD_CK(s, state_to_host(pos4, (const real*)v.pos, N, 4, v, st));
+  if (prev4) UPBD_CK(s, state_to_host(prev4, (const real*)v.prev, N, 4, v, st));
+  if (vel4) UPBD_CK(s, state_to_host(vel4, (const real*)v.vel, N, 4, v, st));
+  if (density2) UPBD_CK(s, state_to_host(density2, (const real*)v.density, N, 2, v, st));
   if (flags) UPBD_CK(s, cudaMemcpyAsync(flags, s->v.flags, N * 4, cudaMemcpyDeviceToHost, st));
   UPBD_CK(s, cudaStreamSynchronize(st));
   return UPBD_OK;
@@ -955,7 +956,7 @@ int upbd_read_state_async(upbd_sim* s, float* pos4, uint32_t* flags) {
   cudaStream_t st = s->stream;
   // the staging copy may still be on its way to the host from the last call
   UPBD_CK(s, cudaStreamWaitEvent(st, s->rb_done, 0));
-  if (pos4) UPBD_CK(s, cudaMemcpyAsync(spos, s->v.pos, N * 16, cudaMemcpyDeviceToDevice, st));
+  if (pos4) UPBD_CK(s, state_to_f32((float*)spos, (const real*)s->v.pos, N, 4, st));
   if (flags) UPBD_CK(s, cudaMemcpyAsync(sflags, s->v.flags, N * 4, cudaMemcpyDeviceToDevice, st));
   UPBD_CK(s, cudaEventRecord(s->rb_ready, st));
   UPBD_CK(s, cudaStreamWaitEvent(s->rb_stream, s->rb_ready, 0));
@@ -979,10 +980,11 @@ int upbd_write_state(upbd_sim* s, const float* pos4, const float* prev4, const f
   cudaSetDevice(s->device);
   const size_t N = (size_t)s->v.N;
   cudaStream_t st = s->stream;
-  if (pos4) UPBD_CK(s, cudaMemcpyAsync(s->v.pos, pos4, N * 16, cudaMemcpyHostToDevice, st));
-  if (prev4) UPBD_CK(s, cudaMemcpyAsync(s->v.prev, prev4, N * 16, cudaMemcpyHostToDevice, st));
-  if (vel4) UPBD_CK(s, cudaMemcpyAsync(s->v.vel, vel4, N * 16, cudaMemcpyHostToDevice, st));
-  if (density2) UPBD_CK(s, cudaMemcpyAsync(s->v.density, density2, N * 8, cudaMemcpyHostToDevice, st));
+  const SimView& v = s->v;
+  if (pos4) UPBD_CK(s, state_to_device((real*)v.pos, pos4, N, 4, v, st));
+  if (prev4) UPBD_CK(s, state_to_device((real*)v.prev, prev4, N, 4, v, st));
+  if (vel4) UPBD_CK(s, state_to_device((real*)v.vel, vel4, N, 4, v, st));
+  if (density2) UPBD_CK(s, state_to_device((real*)v.density, density2, N, 2, v, st));
   if (flags) UPBD_CK(s, cudaMemcpyAsync(s->v.flags, flags, N * 4, cudaMemcpyHostToDevice, st));
   UPBD_CK(s, cudaStreamSynchronize(st));
   return UPBD_OK;
@@ -1172,6 +1174,9 @@ __global__ void k_counts_from_offsets(const uint32_t* __restrict__ offsets, uint
 
 int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t table_size, double cell_size,
                     void* counts, void* offsets, void* entries, void* stream) {
+#ifdef UPBD_FP64_BUILD
+  return fail(nullptr, UPBD_ERR_INVALID, "the stateless grid build reads float rows: not in the FP64 build");
+#endif
   if (n < 0 || (n > 0 && (!pos4 || !flags || !entries)) || !offsets)
     return fail(nullptr, UPBD_ERR_INVALID, "bad grid_build arguments");
   if (table_size < 1 || (table_size & (table_size - 1)) || table_size > (1 << 28))
@@ -1203,7 +1208,7 @@ int upbd_grid_build(const void* pos4, const void* flags, int32_t n, int32_t tabl
   const GridScratchLayout lay = grid_scratch_layout(pd.n_cap, pd.t_cap, sizeof(DevParams));
   uint32_t* w = (uint32_t*)pd.mem;
   SimView v{};
-  v.pos = (float4*)pos4;
+  v.pos = (real4*)pos4;
   v.flags = (uint32_t*)flags;
   v.N = n;
   v.T = table_size;
@@ -1366,6 +1371,9 @@ __global__ void k_noalloc_params(DevParams* p, double inv_cell) { p->inv_cell = 
 extern "C" int upbd_grid_build_noalloc(const void* pos4, const void* flags, int32_t n, int32_t table_size,
                                        double cell_size, void* counts, void* offsets, void* entries,
                                        void* stream) {
+#ifdef UPBD_FP64_BUILD
+  return fail(nullptr, UPBD_ERR_INVALID, "the stateless grid build reads float rows: not in the FP64 build");
+#endif
   if (n < 0 || (n > 0 && (!pos4 || !flags || !entries)) || !offsets)
     return fail(nullptr, UPBD_ERR_INVALID, "bad grid_build_noalloc arguments");
   if (table_size < 1 || (table_size & (table_size - 1)))
@@ -1395,7 +1403,7 @@ extern "C" int upbd_grid_build_noalloc(const void* pos4, const void* flags, int3
   cudaStream_t st = (cudaStream_t)stream;
   const int tiles = (table_size + SCAN_TILE - 1) / SCAN_TILE;
   SimView v{};
-  v.pos = (float4*)pos4;
+  v.pos = (real4*)pos4;
   v.flags = (uint32_t*)flags;
   v.N = n;
   v.T = table_size;

@@ -1,7 +1,8 @@
 // Device-side types and helpers of the unified-particle step (sm_100a).
 //
 // State layout in HBM (structure of arrays, 16-byte aligned rows, the field
-// meanings of src/gpu/wgsl.js:92-98):
+// meanings of src/gpu/wgsl.js:92-98; float4/float2 rows are `real` rows, which
+// are double4/double2 in the test-only FP64 build):
 //   pos[N]     float4  xyz + inverse mass
 //   prev[N]    float4  xyz + grab target x
 //   vel[N]     float4  xyz + grab target y
@@ -39,6 +40,42 @@ constexpr int HM_ACTIVE = 0;
 constexpr int HM_HEALTH = 1;
 constexpr int HM_WORDS = 8;
 
+// Scalar type of the particle state and of the pass arithmetic: float in
+// the product and parity builds (the reference's f32 buffers); double in the
+// test-only FP64 build (UPBD_FP64_BUILD), which instantiates these same pass
+// bodies on double as the reference trajectory for long-run drift. The
+// uniforms, the constraint rest lengths (float bits in cons.z, the buffer
+// layout of the reference), tet rest volumes and the movement bounds stay
+// float in every build.
+#ifdef UPBD_FP64_BUILD
+using real = double;
+using real2 = double2;
+using real4 = double4;
+__host__ __device__ __forceinline__ real4 make_real4(real x, real y, real z, real w) { return make_double4(x, y, z, w); }
+__host__ __device__ __forceinline__ real2 make_real2(real x, real y) { return make_double2(x, y); }
+#else
+using real = float;
+using real2 = float2;
+using real4 = float4;
+__host__ __device__ __forceinline__ real4 make_real4(real x, real y, real z, real w) { return make_float4(x, y, z, w); }
+__host__ __device__ __forceinline__ real2 make_real2(real x, real y) { return make_float2(x, y); }
+#endif
+// Math on the scalar type: the float overloads call exactly what the FP32
+// builds always called.
+__device__ __forceinline__ float r_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double r_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float r_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double r_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float r_fabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double r_fabs(double x) { return fabs(x); }
+__device__ __forceinline__ float r_fmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double r_fmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float r_fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double r_fdiv(double a, double b) { return a / b; }
+// a float no smaller than x (movement bounds kept as float bits); x >= 0
+__device__ __forceinline__ float r_to_float_up(float x) { return x; }
+__device__ __forceinline__ float r_to_float_up(double x) { return __double2float_ru(x); }
+
 // Uniforms of one frame (Params of src/gpu/wgsl.js:36-90), in device memory
 // so captured graphs read the values current at replay.
 struct DevParams {
@@ -66,11 +103,11 @@ struct DevParams {
 
 // Device pointers and sizes of one scene (passed by value to kernels).
 struct SimView {
-  float4* pos;
-  float4* prev;
-  float4* vel;
-  float4* delta;
-  float2* density;
+  real4* pos;
+  real4* prev;
+  real4* vel;
+  real4* delta;
+  real2* density;
   uint32_t* flags;
   uint4* cons;
   const uint32_t* adj;
@@ -87,9 +124,9 @@ struct SimView {
   // Bucket-ordered copies, slot e matching entries[e]: neighbour gathers read
   // a candidate's data with one load at its slot instead of entries -> pos.
   // Every pass that moves a particle also writes its slot's copy.
-  float4* spos;        // position + inverse mass
-  float2* sdens;       // (rho, rho_near) of the density pass
-  float4* svel;        // velocity after velocityUpdate
+  real4* spos;         // position + inverse mass
+  real2* sdens;        // (rho, rho_near) of the density pass
+  real4* svel;         // velocity after velocityUpdate
   uint32_t* slot;      // slot of particle i in this substep's grid
   // Inside a bucket, entries run in descending index, so fluid (indices >= S)
   // precede solids: fend[h] splits bucket h into [start[h], fend[h]) fluid and
@@ -110,15 +147,18 @@ struct SimView {
   const uint32_t* adj_other;  // CSR-parallel: the other endpoint of constraint ids[k]
   const float* adj_scale;     // CSR-parallel: 1 / max(deg_i, deg_other) (static)
   uint32_t* mark;      // per particle: a solid is within contact range (fluid only)
-  float4* sbuf;        // 2 x S: solid positions between folded solve iterations
+  real4* sbuf;         // 2 x S: solid positions between folded solve iterations
   // Slot-ordered fluid positions after applyDeltaFluid: the contact passes
   // (marks, solid-fluid contacts) read the fluid there, while spos keeps the
   // positions the fluid gathers saw until the bounds pass rewrites it.
-  float4* sfp;
+  real4* sfp;
   uint32_t* ccount;
   uint32_t* clist;
   uint32_t* scratch;
   uint32_t* host_mapped;
+#ifdef UPBD_FP64_BUILD
+  float* conv;  // N x 4 floats: host rows staged on their way to or from the double state
+#endif
   int S, N1, dim1, dim2, F, N, C, NT, T, num_tiles;
 };
 
@@ -140,7 +180,7 @@ __device__ __forceinline__ int32_t js_toint32(double x) {
 // products in double, ToInt32, xor, mask.
 struct CellHash {
   int32_t hx[3], hy[3], hz[3];
-  __device__ __forceinline__ void init(float px, float py, float pz, double inv) {
+  __device__ __forceinline__ void init(real px, real py, real pz, double inv) {
     const double cx = floor(__dmul_rn((double)px, inv));
     const double cy = floor(__dmul_rn((double)py, inv));
     const double cz = floor(__dmul_rn((double)pz, inv));
@@ -196,7 +236,7 @@ constexpr float XMOVE_REC = 0.25f;
 constexpr uint32_t NBR_IN = 0x80000000u;  // list entry flag: within H at density time (slots stay below 2^31)
 
 template <int G = GL>
-__device__ __forceinline__ float lane_sum(float x) {
+__device__ __forceinline__ real lane_sum(real x) {
 #pragma unroll
   for (int d = G / 2; d > 0; d >>= 1) x = x + __shfl_xor_sync(0xffffffffu, x, d);
   return x;
@@ -207,7 +247,7 @@ __device__ __forceinline__ float lane_sum(float x) {
 // shuffles. Every lane of the warp must call it (inactive groups pass any
 // position).
 template <int G = GL>
-__device__ __forceinline__ void group_cell_hash(float px, float py, float pz, double inv, CellHash& ch) {
+__device__ __forceinline__ void group_cell_hash(real px, real py, real pz, double inv, CellHash& ch) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & (G - 1);
   const int base = (threadIdx.x & 31) & ~(G - 1);
@@ -217,7 +257,7 @@ __device__ __forceinline__ void group_cell_hash(float px, float py, float pz, do
   for (int m = 0; m < (9 + G - 1) / G; m++) {
     const int j = lane + G * m;
     const int axis = (j < 9) ? j / 3 : 2;
-    const float pa = (axis == 0) ? px : ((axis == 1) ? py : pz);
+    const real pa = (axis == 0) ? px : ((axis == 1) ? py : pz);
     const double K = (axis == 0) ? 92837111.0 : ((axis == 1) ? 689287499.0 : 283923481.0);
     const double c = floor(__dmul_rn((double)pa, inv));
     mine[m] = js_toint32(__dmul_rn(__dadd_rn(c, (double)(j - 3 * axis - 1)), K));
@@ -401,8 +441,9 @@ __device__ __forceinline__ float approx_sqrt(float x) {
   asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+__device__ __forceinline__ double approx_sqrt(double x) { return sqrt(x); }
 
-__device__ __forceinline__ uint32_t cell_of(float px, float py, float pz, double inv, uint32_t mask) {
+__device__ __forceinline__ uint32_t cell_of(real px, real py, real pz, double inv, uint32_t mask) {
   const double cx = floor(__dmul_rn((double)px, inv));
   const double cy = floor(__dmul_rn((double)py, inv));
   const double cz = floor(__dmul_rn((double)pz, inv));
@@ -414,11 +455,11 @@ __device__ __forceinline__ uint32_t cell_of(float px, float py, float pz, double
 
 // std::max / std::min / clamp with the operand order of the oracle (so -0.0
 // and NaN resolve the same way on both sides).
-__device__ __forceinline__ float mx(float a, float b) { return (a < b) ? b : a; }
-__device__ __forceinline__ float mn(float a, float b) { return (b < a) ? b : a; }
-__device__ __forceinline__ float clampf(float e, float lo, float hi) { return mn(mx(e, lo), hi); }
-__device__ __forceinline__ float signf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
-__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+__device__ __forceinline__ real mx(real a, real b) { return (a < b) ? b : a; }
+__device__ __forceinline__ real mn(real a, real b) { return (b < a) ? b : a; }
+__device__ __forceinline__ real clampf(real e, real lo, real hi) { return mn(mx(e, lo), hi); }
+__device__ __forceinline__ real signf(real x) { return x > 0 ? real(1) : (x < 0 ? real(-1) : real(0)); }
+__device__ __forceinline__ real dot3(real ax, real ay, real az, real bx, real by, real bz) {
   return ax * bx + ay * by + az * bz;
 }
 

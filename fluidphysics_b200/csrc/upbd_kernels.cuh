@@ -15,27 +15,27 @@ __global__ void __launch_bounds__(64) k_emit(SimView v, const DevParams* __restr
   if (k >= P->emit_count) return;
   const int slot = v.S + (int)((P->emit_start + k) % (uint32_t)v.F);
   const float4 E_pos = P->emit_pos, E_dir = P->emit_dir, E_side = P->emit_side, E_up = P->emit_up;
-  const float phase = E_dir.w + (float)k * 2.39996f;
-  const float spacing = P->fluid_radius * 2.2f;
-  const float fk = (float)k * 0.618034f;
-  const float rad = spacing * (0.4f + 1.6f * (fk - floorf(fk)));
-  const float c = cosf(phase), s = sinf(phase);
-  const float along = (float)(k % 8u) * spacing * 0.5f;
-  const float offx = E_side.x * (c * rad) + E_up.x * (s * rad) + E_dir.x * along;
-  const float offy = E_side.y * (c * rad) + E_up.y * (s * rad) + E_dir.y * along;
-  const float offz = E_side.z * (c * rad) + E_up.z * (s * rad) + E_dir.z * along;
-  const float px = E_pos.x + offx, py = E_pos.y + offy, pz = E_pos.z + offz;
-  const float a = sinf(phase * 12.9898f) * 43758.547f;
-  const float b = sinf(phase * 78.233f) * 12543.123f;
-  const float d = sinf(phase * 39.425f) * 26781.897f;
-  const float jx = ((a - floorf(a)) - 0.5f) * 0.5f;
-  const float jy = ((b - floorf(b)) - 0.5f) * 0.5f;
-  const float jz = ((d - floorf(d)) - 0.5f) * 0.5f;
-  const float speed = E_pos.w;
-  const float w = v.pos[slot].w;
-  v.pos[slot] = make_float4(px, py, pz, w);
-  v.prev[slot] = make_float4(px, py, pz, 0.f);
-  v.vel[slot] = make_float4(E_dir.x * speed + jx, E_dir.y * speed + jy, E_dir.z * speed + jz, 0.f);
+  const real phase = E_dir.w + (real)k * 2.39996f;
+  const real spacing = P->fluid_radius * 2.2f;
+  const real fk = (real)k * 0.618034f;
+  const real rad = spacing * (0.4f + 1.6f * (fk - floorf(fk)));
+  const real c = cosf(phase), s = sinf(phase);
+  const real along = (real)(k % 8u) * spacing * 0.5f;
+  const real offx = E_side.x * (c * rad) + E_up.x * (s * rad) + E_dir.x * along;
+  const real offy = E_side.y * (c * rad) + E_up.y * (s * rad) + E_dir.y * along;
+  const real offz = E_side.z * (c * rad) + E_up.z * (s * rad) + E_dir.z * along;
+  const real px = E_pos.x + offx, py = E_pos.y + offy, pz = E_pos.z + offz;
+  const real a = sinf(phase * 12.9898f) * 43758.547f;
+  const real b = sinf(phase * 78.233f) * 12543.123f;
+  const real d = sinf(phase * 39.425f) * 26781.897f;
+  const real jx = ((a - floorf(a)) - 0.5f) * 0.5f;
+  const real jy = ((b - floorf(b)) - 0.5f) * 0.5f;
+  const real jz = ((d - floorf(d)) - 0.5f) * 0.5f;
+  const real speed = E_pos.w;
+  const real w = v.pos[slot].w;
+  v.pos[slot] = make_real4(px, py, pz, w);
+  v.prev[slot] = make_real4(px, py, pz, 0.f);
+  v.vel[slot] = make_real4(E_dir.x * speed + jx, E_dir.y * speed + jy, E_dir.z * speed + jz, 0.f);
   v.flags[slot] = F_ACTIVE;
 }
 
@@ -45,10 +45,10 @@ __global__ void k_emit_particles(SimView v, const float* __restrict__ p3,
   const int k = UPBD_TID;
   if (k >= n) return;
   const int slot = v.S + (int)(((long long)start + k) % v.F);
-  const float x = p3[3 * k], y = p3[3 * k + 1], z = p3[3 * k + 2];
-  v.pos[slot] = make_float4(x, y, z, inv_mass);
-  v.prev[slot] = make_float4(x, y, z, 0.f);
-  v.vel[slot] = make_float4(v3[3 * k], v3[3 * k + 1], v3[3 * k + 2], 0.f);
+  const real x = p3[3 * k], y = p3[3 * k + 1], z = p3[3 * k + 2];
+  v.pos[slot] = make_real4(x, y, z, inv_mass);
+  v.prev[slot] = make_real4(x, y, z, 0.f);
+  v.vel[slot] = make_real4(v3[3 * k], v3[3 * k + 1], v3[3 * k + 2], 0.f);
   v.flags[slot] = F_ACTIVE;
 }
 
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) k_cut(SimView v, const DevParams* __restr
   const double nz = __dsub_rn(__dmul_rn(d1x, d2y), __dmul_rn(d1y, d2x));
   const double nl = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(nx, nx), __dmul_rn(ny, ny)), __dmul_rn(nz, nz)));
   if (nl < 1e-8) return;
-  const float4 A = v.pos[cc.x], B = v.pos[cc.y];
+  const real4 A = v.pos[cc.x], B = v.pos[cc.y];
   const double ax = A.x, ay = A.y, az = A.z, bx = B.x, by = B.y, bz = B.z;
   const double sa = __dadd_rn(__dadd_rn(__dmul_rn(__dsub_rn(ax, ox), nx), __dmul_rn(__dsub_rn(ay, oy), ny)),
                               __dmul_rn(__dsub_rn(az, oz), nz));
@@ -154,26 +154,26 @@ __global__ void __launch_bounds__(256) k_cut(SimView v, const DevParams* __restr
 __global__ void __launch_bounds__(256) k_cut_tets(SimView v, const DevParams* __restrict__ P) {
   const int t = UPBD_TID;
   if (t >= v.NT) return;
-  const float V0 = v.tet_vol[t];
+  const real V0 = v.tet_vol[t];
   if (V0 <= 0.f) return;
-  const float ox = (float)P->cut_o[0], oy = (float)P->cut_o[1], oz = (float)P->cut_o[2];
-  const float ax1 = (float)P->cut_d1[0], ay1 = (float)P->cut_d1[1], az1 = (float)P->cut_d1[2];
-  const float ax2 = (float)P->cut_d2[0], ay2 = (float)P->cut_d2[1], az2 = (float)P->cut_d2[2];
-  float nx, ny, nz;
+  const real ox = (real)P->cut_o[0], oy = (real)P->cut_o[1], oz = (real)P->cut_o[2];
+  const real ax1 = (real)P->cut_d1[0], ay1 = (real)P->cut_d1[1], az1 = (real)P->cut_d1[2];
+  const real ax2 = (real)P->cut_d2[0], ay2 = (real)P->cut_d2[1], az2 = (real)P->cut_d2[2];
+  real nx, ny, nz;
   cross3(ax1, ay1, az1, ax2, ay2, az2, nx, ny, nz);
   if (dot3(nx, ny, nz, nx, ny, nz) < 1e-16f) return;
   for (int p = 0; p < 3; p++)
     for (int q = p + 1; q < 4; q++) {
-      const float4 A = v.pos[v.tet_idx[4 * t + p]];
-      const float4 B = v.pos[v.tet_idx[4 * t + q]];
-      const float pax = A.x - ox, pay = A.y - oy, paz = A.z - oz;
-      const float pbx = B.x - ox, pby = B.y - oy, pbz = B.z - oz;
-      const float sa = dot3(pax, pay, paz, nx, ny, nz);
-      const float sb = dot3(pbx, pby, pbz, nx, ny, nz);
+      const real4 A = v.pos[v.tet_idx[4 * t + p]];
+      const real4 B = v.pos[v.tet_idx[4 * t + q]];
+      const real pax = A.x - ox, pay = A.y - oy, paz = A.z - oz;
+      const real pbx = B.x - ox, pby = B.y - oy, pbz = B.z - oz;
+      const real sa = dot3(pax, pay, paz, nx, ny, nz);
+      const real sb = dot3(pbx, pby, pbz, nx, ny, nz);
       if (sa * sb >= 0.f) continue;
-      const float tt = sa / (sa - sb);
-      const float ppx = pax + (pbx - pax) * tt, ppy = pay + (pby - pay) * tt, ppz = paz + (pbz - paz) * tt;
-      float cx, cy, cz;
+      const real tt = sa / (sa - sb);
+      const real ppx = pax + (pbx - pax) * tt, ppy = pay + (pby - pay) * tt, ppz = paz + (pbz - paz) * tt;
+      real cx, cy, cz;
       cross3(ax1, ay1, az1, ppx, ppy, ppz, cx, cy, cz);
       if (dot3(cx, cy, cz, nx, ny, nz) < 0.f) continue;
       cross3(ppx, ppy, ppz, ax2, ay2, az2, cx, cy, cz);
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(256) k_cut_tets(SimView v, const DevParams* __
 // double). t >= 0, so its IEEE bits order like unsigned integers.
 __device__ __forceinline__ bool pick_t(const SimView& v, const DevParams* __restrict__ P, int i, double& t) {
   if (!(v.flags[i] & F_ACTIVE)) return false;
-  const float4 p = v.pos[i];
+  const real4 p = v.pos[i];
   const double ox = P->pick_o[0], oy = P->pick_o[1], oz = P->pick_o[2], mp = P->pick_o[3];
   const double dx = P->pick_d[0], dy = P->pick_d[1], dz = P->pick_d[2];
   const double px = __dsub_rn((double)p.x, ox), py = __dsub_rn((double)p.y, oy), pz = __dsub_rn((double)p.z, oz);
@@ -233,15 +233,15 @@ __global__ void __launch_bounds__(256) k_grab_select(SimView v, const DevParams*
   const uint32_t lat = (i >= v.N1) ? 1u : 0u;
   if (P->grab_lattice != 0xffffu && lat != P->grab_lattice) return;
   const float4 c = P->grab_c;
-  const float4 p = v.pos[i];
-  const float dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
-  const float q2 = dot3(dx, dy, dz, dx, dy, dz) / (c.w * c.w);
+  const real4 p = v.pos[i];
+  const real dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+  const real q2 = dot3(dx, dy, dz, dx, dy, dz) / (c.w * c.w);
   if (q2 < 1.0f) {
     v.flags[i] = f | F_GRABBED;
-    const float w = (1.0f - q2) * (1.0f - q2) * 0.95f + 0.05f;
+    const real w = (1.0f - q2) * (1.0f - q2) * 0.95f + 0.05f;
     v.prev[i].w = p.x;
     v.vel[i].w = p.y;
-    v.density[i] = make_float2(p.z, w);
+    v.density[i] = make_real2(p.z, w);
   }
 }
 
@@ -254,12 +254,12 @@ __global__ void k_grab_indices(SimView v, const uint32_t* __restrict__ idx, cons
   if (i >= (uint32_t)v.S) return;
   const uint32_t f = v.flags[i];
   if (!(f & F_ACTIVE)) return;
-  const float4 p = v.pos[i];
-  const float tx = t3 ? t3[3 * k] : p.x, ty = t3 ? t3[3 * k + 1] : p.y, tz = t3 ? t3[3 * k + 2] : p.z;
+  const real4 p = v.pos[i];
+  const real tx = t3 ? t3[3 * k] : p.x, ty = t3 ? t3[3 * k + 1] : p.y, tz = t3 ? t3[3 * k + 2] : p.z;
   v.flags[i] = f | F_GRABBED;
   v.prev[i].w = tx;
   v.vel[i].w = ty;
-  v.density[i] = make_float2(tz, w ? w[k] : 1.0f);
+  v.density[i] = make_real2(tz, w ? w[k] : 1.0f);
 }
 
 // grabRelease, src/gpu/wgsl.js:867-871

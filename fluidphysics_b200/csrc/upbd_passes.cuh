@@ -3,7 +3,9 @@
 // and keeps their floating-point operand order; passes that only touch a
 // particle's own slot are fused into one body. All of them are FP32 SIMT
 // gathers over HBM-resident state: there is no dense contraction on this
-// path, so the tensor cores have no role here.
+// path, so the tensor cores have no role here. The scalar type is `real`
+// (upbd_device.cuh): float, or double in the test-only FP64 build that
+// re-runs these same bodies as the drift reference.
 //
 // A body processes one block-sized tile `vb` of one scene (thread index
 // vb * blockDim.x + threadIdx.x). The single-scene kernels (upbd_kernels.cuh)
@@ -27,48 +29,48 @@ __device__ __forceinline__ void b_integrate_count(const SimView& v, const DevPar
   if (i >= v.N) return;
   uint32_t f = v.flags[i];
   if (!(f & F_ACTIVE)) return;
-  float4 p4 = v.pos[i];
+  real4 p4 = v.pos[i];
   if (INTEGRATE) {
-    const float h = P->h;
-    const float4 vv = v.vel[i];
-    const float vx = vv.x, vz = vv.z;
-    const float vy = vv.y + P->gravity * h;
-    const float px = p4.x, py = p4.y, pz = p4.z;
-    float nx = px + vx * h, ny = py + vy * h, nz = pz + vz * h;
-    const float4 pv = v.prev[i];
-    float tw = pv.w;
+    const real h = P->h;
+    const real4 vv = v.vel[i];
+    const real vx = vv.x, vz = vv.z;
+    const real vy = vv.y + P->gravity * h;
+    const real px = p4.x, py = p4.y, pz = p4.z;
+    real nx = px + vx * h, ny = py + vy * h, nz = pz + vz * h;
+    const real4 pv = v.prev[i];
+    real tw = pv.w;
     bool slipped = false;
     if (f & F_GRABBED) {
       const float4 gd = P->grab_delta;
-      const float2 dn = v.density[i];
-      float tx = pv.w, ty = vv.w, tz = dn.x;
+      const real2 dn = v.density[i];
+      real tx = pv.w, ty = vv.w, tz = dn.x;
       tx = tx + gd.x; ty = ty + gd.y; tz = tz + gd.z;
-      const float ex = nx - tx, ey = ny - ty, ez = nz - tz;
-      if (sqrtf(dot3(ex, ey, ez, ex, ey, ez)) > 1.0f) {
+      const real ex = nx - tx, ey = ny - ty, ez = nz - tz;
+      if (r_sqrt(dot3(ex, ey, ez, ex, ey, ez)) > 1.0f) {
         f &= ~F_GRABBED;
         v.flags[i] = f;
-        v.vel[i] = make_float4(vx, vy, vz, 0.f);
+        v.vel[i] = make_real4(vx, vy, vz, 0.f);
         slipped = true;
       } else {
-        const float k = P->grab_k * dn.y;
-        float cx = (tx - nx) * k, cy = (ty - ny) * k, cz = (tz - nz) * k;
-        const float cl = sqrtf(dot3(cx, cy, cz, cx, cy, cz));
-        const float maxC = 0.05f;
+        const real k = P->grab_k * dn.y;
+        real cx = (tx - nx) * k, cy = (ty - ny) * k, cz = (tz - nz) * k;
+        const real cl = r_sqrt(dot3(cx, cy, cz, cx, cy, cz));
+        const real maxC = 0.05f;
         if (cl > maxC) {
-          const float g = maxC / cl;
+          const real g = maxC / cl;
           cx = cx * g; cy = cy * g; cz = cz * g;
         }
         nx = nx + cx; ny = ny + cy; nz = nz + cz;
         tw = tx;
-        v.vel[i] = make_float4(vx, vy, vz, ty);
-        v.density[i] = make_float2(tz, dn.y);
+        v.vel[i] = make_real4(vx, vy, vz, ty);
+        v.density[i] = make_real2(tz, dn.y);
       }
     } else {
-      v.vel[i] = make_float4(vx, vy, vz, vv.w);
+      v.vel[i] = make_real4(vx, vy, vz, vv.w);
     }
     (void)slipped;
-    v.prev[i] = make_float4(px, py, pz, tw);
-    p4 = make_float4(nx, ny, nz, p4.w);
+    v.prev[i] = make_real4(px, py, pz, tw);
+    p4 = make_real4(nx, ny, nz, p4.w);
     v.pos[i] = p4;
     if (i >= v.S) v.mark[i] = 0u;  // contact marks of this substep start clear
   }
@@ -233,38 +235,38 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   bool act;
   slot_group(v, t, myslot, i, act);
   if (!__any_sync(0xffffffffu, act)) return;  // a warp of solid slots (or past the active count)
-  float rho = 0.f, rhoNear = 0.f;
-  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
+  real rho = 0.f, rhoNear = 0.f;
+  const real4 pi = act ? v.spos[myslot] : make_real4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash<GLF>(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  const float H = P->fluid_h, H2 = H * H;
-  const float HS = H * (1.0f + XSKIN), HS2 = HS * HS;  // list radius (for xsph)
-  const float4* __restrict__ spos = v.spos;
+  const real H = P->fluid_h, H2 = H * H;
+  const real HS = H * (1.0f + XSKIN), HS2 = HS * HS;  // list radius (for xsph)
+  const real4* __restrict__ spos = v.spos;
   // lane l's c-th listed candidate goes to row l*NL + c, column myslot
   const uint32_t NS = (uint32_t)v.N;
   uint32_t* __restrict__ nbr = v.nbr + (size_t)lane * NL * NS + myslot;
   uint32_t cnt = 0;
 #ifndef UPBD_PARITY_BUILD
-  const float invH = 1.0f / H;
+  const real invH = 1.0f / H;
 #endif
-  lane_strided<0, GLF>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const float4& pj) {
-    const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+  lane_strided<0, GLF>(v, ch, lane, act, [&](uint32_t e) { return spos[e]; }, [&](uint32_t e, const real4& pj) {
+    const real ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+    const real d2 = dot3(ex, ey, ez, ex, ey, ez);
 #ifdef UPBD_PARITY_BUILD
     if (e == myslot) return;
     if (d2 >= HS2) return;
     if (cnt < NL) nbr[cnt * NS] = e | ((d2 < H2) ? NBR_IN : 0u);  // for fluidDisp (same positions) and xsph
     cnt++;
     if (d2 >= H2) return;
-    const float q = 1.0f - sqrtf(d2) / H;
+    const real q = 1.0f - r_sqrt(d2) / H;
     rho = rho + q * q;
     rhoNear = rhoNear + q * q * q;
 #else
     // branch-free: every lane of the warp takes the same path per candidate
     const bool in = (e != myslot) && (d2 < H2);
     const bool listed = (e != myslot) && (d2 < HS2);
-    const float q = 1.0f - approx_sqrt(d2) * invH;
-    const float qq = in ? q * q : 0.0f;
+    const real q = 1.0f - approx_sqrt(d2) * invH;
+    const real qq = in ? q * q : 0.0f;
     rho = rho + qq;
     rhoNear = rhoNear + qq * q;
     if (listed && cnt < NL) nbr[cnt * NS] = e | (in ? NBR_IN : 0u);  // for fluidDisp (same positions) and xsph
@@ -275,7 +277,7 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   rho = lane_sum<GLF>(rho);
   rhoNear = lane_sum<GLF>(rhoNear);
   if (act && lane == 0) {
-    const float2 d = make_float2(rho, rhoNear);
+    const real2 d = make_real2(rho, rhoNear);
     v.density[i] = d;
     v.sdens[myslot] = d;
   }
@@ -303,40 +305,40 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
   } else if (!act) {
     return;
   }
-  const float H = P->fluid_h, H2 = H * H;
-  float sx = 0.f, sy = 0.f, sz = 0.f;
-  const float4* __restrict__ spos = v.spos;
-  const float2* __restrict__ sdens = v.sdens;
-  const float4 pi = act ? spos[e0] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const real H = P->fluid_h, H2 = H * H;
+  real sx = 0.f, sy = 0.f, sz = 0.f;
+  const real4* __restrict__ spos = v.spos;
+  const real2* __restrict__ sdens = v.sdens;
+  const real4 pi = act ? spos[e0] : make_real4(0.f, 0.f, 0.f, 0.f);
   if (act) {
-    const float maxPair = 0.05f * H;
-    const float k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
-    const float2 di = sdens[e0];
-    const float Pi = k * (di.x - rho0);
-    const float PNi = kn * di.y;
+    const real maxPair = 0.05f * H;
+    const real k = P->stiffness, kn = P->near_stiffness, rho0 = P->rest_density;
+    const real2 di = sdens[e0];
+    const real Pi = k * (di.x - rho0);
+    const real PNi = kn * di.y;
 #ifndef UPBD_PARITY_BUILD
-    const float invH = 1.0f / H;
+    const real invH = 1.0f / H;
 #endif
-    auto pair = [&](const float4& pj, const float2& dj) {
-      const float ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
-      const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+    auto pair = [&](const real4& pj, const real2& dj) {
+      const real ex = pj.x - pi.x, ey = pj.y - pi.y, ez = pj.z - pi.z;
+      const real d2 = dot3(ex, ey, ez, ex, ey, ez);
       if (d2 >= H2 || d2 < 1e-12f) return;
 #ifdef UPBD_PARITY_BUILD
-      const float d = sqrtf(d2);
-      const float q = 1.0f - d / H;
+      const real d = r_sqrt(d2);
+      const real q = 1.0f - d / H;
 #else
-      const float rd = rsqrtf(d2);  // d2 >= 1e-12 here
-      const float d = d2 * rd;
-      const float q = 1.0f - d * invH;
+      const real rd = r_rsqrt(d2);  // d2 >= 1e-12 here
+      const real d = d2 * rd;
+      const real q = 1.0f - d * invH;
 #endif
-      const float Pj = k * (dj.x - rho0);
-      const float PNj = kn * dj.y;
-      float D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
+      const real Pj = k * (dj.x - rho0);
+      const real PNj = kn * dj.y;
+      real D = 0.25f * ((Pi + Pj) * q + (PNi + PNj) * q * q);
       D = clampf(D, -maxPair, maxPair);
 #ifdef UPBD_PARITY_BUILD
-      const float f = D / d;
+      const real f = D / d;
 #else
-      const float f = D * rd;
+      const real f = D * rd;
 #endif
       sx = sx - ex * f; sy = sy - ey * f; sz = sz - ez * f;
     };
@@ -357,8 +359,8 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
         // in flight together (a lane list holds ~4)
         for (uint32_t c = 0; c < cnt[u]; c += 4) {
           uint32_t e[4];
-          float4 pj[4];
-          float2 dj[4];
+          real4 pj[4];
+          real2 dj[4];
 #pragma unroll
           for (int w = 0; w < 4; w++) {
             // entries beyond H (listed for xsph) and past the count become the
@@ -399,18 +401,18 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
     sz = sz + __shfl_xor_sync(0xffffffffu, sz, d);
   }
   if (!act || h != 0) return;
-  const float maxTotal = 0.35f * H;
-  const float s2 = dot3(sx, sy, sz, sx, sy, sz);
+  const real maxTotal = 0.35f * H;
+  const real s2 = dot3(sx, sy, sz, sx, sy, sz);
   if (s2 > maxTotal * maxTotal) {
-    const float f = maxTotal / sqrtf(s2);
+    const real f = maxTotal / r_sqrt(s2);
     sx = sx * f; sy = sy * f; sz = sz * f;
   }
   if (APPLY) {  // pi is pos[i]: the grid build copied it and nothing moved it since
-    const float4 p = make_float4(pi.x + sx, pi.y + sy, pi.z + sz, pi.w);
+    const real4 p = make_real4(pi.x + sx, pi.y + sy, pi.z + sz, pi.w);
     v.pos[i] = p;
     v.sfp[e0] = p;
   } else {
-    v.delta[i] = make_float4(sx, sy, sz, 1.0f);
+    v.delta[i] = make_real4(sx, sy, sz, 1.0f);
   }
 }
 
@@ -419,8 +421,8 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
   const int i = v.S + (int)UPBD_VTID;
   if (i >= v.N) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
-  float4 p = v.pos[i];
-  const float4 d = v.delta[i];
+  real4 p = v.pos[i];
+  const real4 d = v.delta[i];
   p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
   v.pos[i] = p;
   v.sfp[v.slot[i]] = p;
@@ -433,16 +435,16 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
 // Every lane of the warp calls it (the hash is shared by shuffles); only
 // active solids walk.
 template <int G = GL>
-__device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, float4 p,
+__device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, real4 p,
                                                 bool act, int lane) {
   CellHash ch;
   group_cell_hash<G>(p.x, p.y, p.z, P->inv_cell, ch);
-  const float rsum = P->solid_radius + P->fluid_radius;
-  const float lim2 = rsum * rsum * 1.00001f;
-  const float4* __restrict__ sfp = v.sfp;  // the fluid has moved by its displacement
+  const real rsum = P->solid_radius + P->fluid_radius;
+  const real lim2 = rsum * rsum * 1.00001f;
+  const real4* __restrict__ sfp = v.sfp;  // the fluid has moved by its displacement
   uint32_t* __restrict__ mark = v.mark;
-  lane_strided<0, G>(v, ch, lane, act, [&](uint32_t e) { return sfp[e]; }, [&](uint32_t e, const float4& pj) {
-    const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+  lane_strided<0, G>(v, ch, lane, act, [&](uint32_t e) { return sfp[e]; }, [&](uint32_t e, const real4& pj) {
+    const real ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
     if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
   });
 }
@@ -476,8 +478,8 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
   if (t >= solid_pad) {
     const int i = v.S + (t - solid_pad);
     if (APPLY_FLUID && i < v.N && (v.flags[i] & F_ACTIVE)) {
-      float4 p = v.pos[i];
-      const float4 d = v.delta[i];
+      real4 p = v.pos[i];
+      const real4 d = v.delta[i];
       p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
       v.pos[i] = p;
       v.sfp[v.slot[i]] = p;
@@ -487,13 +489,13 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
   const int i = t / GL;
   const int lane = threadIdx.x & (GL - 1);
   const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
-  const float4* __restrict__ pos = (OUT == SOLVE_DELTA || it == 0) ? v.pos : v.sbuf + (size_t)((it - 1) & 1) * v.S;
-  const float4 pi = (i < v.S) ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  float cx = 0.f, cy = 0.f, cz = 0.f;
+  const real4* __restrict__ pos = (OUT == SOLVE_DELTA || it == 0) ? v.pos : v.sbuf + (size_t)((it - 1) & 1) * v.S;
+  const real4 pi = (i < v.S) ? pos[i] : make_real4(0.f, 0.f, 0.f, 0.f);
+  real cx = 0.f, cy = 0.f, cz = 0.f;
   if (act) {
-    const float wi = pi.w;
-    const float h = P->h;
-    const float alpha = P->compliance / (h * h);
+    const real wi = pi.w;
+    const real h = P->h;
+    const real alpha = P->compliance / (h * h);
     const uint32_t st = v.adj[i], en = v.adj[i + 1];
     const uint32_t* __restrict__ ids = v.adj + v.S + 1;
     const uint4* __restrict__ cons = v.cons;
@@ -501,18 +503,18 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
     for (uint32_t k = st + lane; k < en; k += GL) {
       const uint32_t ci = __ldg(&ids[k]);
       const uint32_t other = __ldg(&v.adj_other[k]);
-      const float s = __ldg(&v.adj_scale[k]);
-      const float4 po = pos[other];
+      const real s = __ldg(&v.adj_scale[k]);
+      const real4 po = pos[other];
       const uint2 rw = *reinterpret_cast<const uint2*>(&cons[ci].z);  // rest bits, alive
       if (rw.y == 0u) continue;
-      const float rest = __uint_as_float(rw.x);
-      const float ex = pi.x - po.x, ey = pi.y - po.y, ez = pi.z - po.z;
-      const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
+      const real rest = __uint_as_float(rw.x);
+      const real ex = pi.x - po.x, ey = pi.y - po.y, ez = pi.z - po.z;
+      const real d = r_sqrt(dot3(ex, ey, ez, ex, ey, ez));
       if (d < 1e-9f) continue;
-      const float wsum = wi + po.w;
+      const real wsum = wi + po.w;
       if (wsum == 0.f) continue;
-      const float dl = -(d - rest) / (wsum + alpha);
-      const float f = dl * wi / d * s;
+      const real dl = -(d - rest) / (wsum + alpha);
+      const real f = dl * wi / d * s;
       cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
     }
   }
@@ -520,12 +522,12 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
   cy = lane_sum(cy);
   cz = lane_sum(cz);
   if (OUT == SOLVE_DELTA) {
-    if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+    if (act && lane == 0) v.delta[i] = make_real4(cx, cy, cz, 1.0f);
     return;
   }
   // applyDeltaSolid on the correction just summed (the delta b_apply_solid reads)
-  const float w = P->omega;
-  float4 p = pi;
+  const real w = P->omega;
+  real4 p = pi;
   if (act) {
     p.x = p.x + cx * w; p.y = p.y + cy * w; p.z = p.z + cz * w;
   }
@@ -537,7 +539,7 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
     v.pos[i] = p;
     v.spos[v.slot[i]] = p;
   }
-  if (OUT == SOLVE_LAST && P->use_mark) mark_fluid_near(v, P, act ? p : make_float4(0.f, 0.f, 0.f, 0.f), act, lane);
+  if (OUT == SOLVE_LAST && P->use_mark) mark_fluid_near(v, P, act ? p : make_real4(0.f, 0.f, 0.f, 0.f), act, lane);
 }
 
 // applyDeltaSolid, src/gpu/wgsl.js:361-366. With MARK (last iteration of the
@@ -549,11 +551,11 @@ __device__ __forceinline__ void b_apply_solid(const SimView& v, const DevParams*
   const int i = MARK ? t / GL : t;
   const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
   if (!MARK && !act) return;
-  const float w = P->omega;
-  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+  const real w = P->omega;
+  real4 p = make_real4(0.f, 0.f, 0.f, 0.f);
   if (act) {
     p = v.pos[i];
-    const float4 d = v.delta[i];
+    const real4 d = v.delta[i];
     p.x = p.x + d.x * w; p.y = p.y + d.y * w; p.z = p.z + d.z * w;
   }
   if (!MARK) {
@@ -578,17 +580,17 @@ __device__ __forceinline__ void b_contact_mark(const SimView& v, const DevParams
   const int t = UPBD_VTID;
   const int i = t / G;
   const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
-  mark_fluid_near<G>(v, P, act ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (G - 1));
+  mark_fluid_near<G>(v, P, act ? v.pos[i] : make_real4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (G - 1));
 }
 
 // latticeRest, src/gpu/wgsl.js:373-381
-__device__ __forceinline__ float lattice_rest(const SimView& v, float spacing, uint32_t a0, uint32_t b0) {
+__device__ __forceinline__ real lattice_rest(const SimView& v, real spacing, uint32_t a0, uint32_t b0) {
   uint32_t a = a0, b = b0, D = (uint32_t)v.dim1;
   if (a0 >= (uint32_t)v.N1) { a = a0 - v.N1; b = b0 - v.N1; D = (uint32_t)(v.dim2 > 1 ? v.dim2 : 1); }
-  const float ax = (float)(a / (D * D)), ay = (float)((a / D) % D), az = (float)(a % D);
-  const float bx = (float)(b / (D * D)), by = (float)((b / D) % D), bz = (float)(b % D);
-  const float dx = ax - bx, dy = ay - by, dz = az - bz;
-  return spacing * sqrtf(dx * dx + dy * dy + dz * dz);
+  const real ax = (real)(a / (D * D)), ay = (real)((a / D) % D), az = (real)(a % D);
+  const real bx = (real)(b / (D * D)), by = (real)((b / D) % D), bz = (real)(b % D);
+  const real dx = ax - bx, dy = ay - by, dz = az - bz;
+  return spacing * r_sqrt(dx * dx + dy * dy + dz * dz);
 }
 
 // latticeAdjacent, src/gpu/wgsl.js:409-416
@@ -611,9 +613,9 @@ __device__ __forceinline__ bool is_bonded(const SimView& v, uint32_t i, uint32_t
   return false;
 }
 
-__device__ __forceinline__ float solid_rsum(const SimView& v, const DevParams* __restrict__ P,
+__device__ __forceinline__ real solid_rsum(const SimView& v, const DevParams* __restrict__ P,
                                             uint32_t i, uint32_t j) {
-  const float rsum = 2.0f * P->solid_radius;
+  const real rsum = 2.0f * P->solid_radius;
   if (lattice_adjacent(v, i, j)) return mn(rsum, P->spacing * 0.97f);
   return rsum;
 }
@@ -624,8 +626,8 @@ __device__ __forceinline__ void b_collect_contacts(const SimView& v, const DevPa
   if (i >= v.S) return;
   uint32_t cnt = 0;
   if (v.flags[i] & F_ACTIVE) {
-    const float4 pi = v.pos[i];
-    const float margin = 2.0f * P->solid_radius;
+    const real4 pi = v.pos[i];
+    const real margin = 2.0f * P->solid_radius;
     const uint32_t mask = (uint32_t)v.T - 1u;
     CellHash ch;
     ch.init(pi.x, pi.y, pi.z, P->inv_cell);
@@ -637,9 +639,9 @@ __device__ __forceinline__ void b_collect_contacts(const SimView& v, const DevPa
           for (uint32_t e = v.start[hb]; e < e1; e++) {
             const uint32_t j = v.entries[e];
             if (j == (uint32_t)i || j >= (uint32_t)v.S || cnt >= C_K) continue;
-            const float4 pj = v.pos[j];
-            const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-            const float lim = solid_rsum(v, P, i, j) + margin;
+            const real4 pj = v.pos[j];
+            const real ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
+            const real lim = solid_rsum(v, P, i, j) + margin;
             if (dot3(ex, ey, ez, ex, ey, ez) >= lim * lim) continue;
             if (is_bonded(v, i, j)) continue;
             v.clist[(size_t)i * C_K + cnt] = j;
@@ -655,24 +657,24 @@ __device__ __forceinline__ void b_solid_contacts(const SimView& v, const DevPara
   const int i = UPBD_VTID;
   if (i >= v.S) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 pi = v.pos[i];
-  const float wi = pi.w;
-  float cx = 0.f, cy = 0.f, cz = 0.f;
+  const real4 pi = v.pos[i];
+  const real wi = pi.w;
+  real cx = 0.f, cy = 0.f, cz = 0.f;
   const uint32_t n = v.ccount[i];
   for (uint32_t k = 0; k < n; k++) {
     const uint32_t j = v.clist[(size_t)i * C_K + k];
-    const float4 pj = v.pos[j];
-    const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-    const float rsum = solid_rsum(v, P, i, j);
-    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+    const real4 pj = v.pos[j];
+    const real ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
+    const real rsum = solid_rsum(v, P, i, j);
+    const real d2 = dot3(ex, ey, ez, ex, ey, ez);
     if (d2 >= rsum * rsum || d2 < 1e-12f) continue;
-    const float wsum = wi + pj.w;
+    const real wsum = wi + pj.w;
     if (wsum == 0.f) continue;
-    const float d = sqrtf(d2);
-    const float f = (rsum - d) / d * wi / wsum * 0.5f;
+    const real d = r_sqrt(d2);
+    const real f = (rsum - d) / d * wi / wsum * 0.5f;
     cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
   }
-  v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+  v.delta[i] = make_real4(cx, cy, cz, 1.0f);
 }
 
 // applySolidContacts, src/gpu/wgsl.js:587-596
@@ -680,22 +682,22 @@ __device__ __forceinline__ void b_apply_solid_contacts(const SimView& v, const D
   const int i = UPBD_VTID;
   if (i >= v.S) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
-  const float maxC = 0.5f * P->solid_radius;
-  const float4 dd = v.delta[i];
-  float dx = dd.x, dy = dd.y, dz = dd.z;
-  const float m2 = dot3(dx, dy, dz, dx, dy, dz);
+  const real maxC = 0.5f * P->solid_radius;
+  const real4 dd = v.delta[i];
+  real dx = dd.x, dy = dd.y, dz = dd.z;
+  const real m2 = dot3(dx, dy, dz, dx, dy, dz);
   if (m2 > maxC * maxC) {
-    const float f = maxC / sqrtf(m2);
+    const real f = maxC / r_sqrt(m2);
     dx = dx * f; dy = dy * f; dz = dz * f;
   }
-  float4 p = v.pos[i];
+  real4 p = v.pos[i];
   p.x = p.x + dx; p.y = p.y + dy; p.z = p.z + dz;
   v.pos[i] = p;
   v.spos[v.slot[i]] = p;
 }
 
-__device__ __forceinline__ void cross3(float ax, float ay, float az, float bx, float by, float bz,
-                                       float& x, float& y, float& z) {
+__device__ __forceinline__ void cross3(real ax, real ay, real az, real bx, real by, real bz,
+                                       real& x, real& y, real& z) {
   x = ay * bz - az * by;
   y = az * bx - ax * bz;
   z = ax * by - ay * bx;
@@ -707,55 +709,55 @@ __device__ __forceinline__ void b_solve_tets(const SimView& v, const DevParams* 
   if (i >= v.S) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
   const uint32_t* ids = v.tet_adj + v.S + 1;
-  float cx = 0.f, cy = 0.f, cz = 0.f;
+  real cx = 0.f, cy = 0.f, cz = 0.f;
   for (uint32_t k = v.tet_adj[i]; k < v.tet_adj[i + 1]; k++) {
     const uint32_t t = ids[k];
     const uint32_t ia = v.tet_idx[4 * t], ib = v.tet_idx[4 * t + 1], ic = v.tet_idx[4 * t + 2],
                    id = v.tet_idx[4 * t + 3];
-    const float V0 = v.tet_vol[t];
+    const real V0 = v.tet_vol[t];
     if (V0 <= 0.f) continue;
-    const float4 pa = v.pos[ia], pb = v.pos[ib], pc = v.pos[ic], pd = v.pos[id];
-    const float bax = pb.x - pa.x, bay = pb.y - pa.y, baz = pb.z - pa.z;
-    const float cax = pc.x - pa.x, cay = pc.y - pa.y, caz = pc.z - pa.z;
-    const float dax = pd.x - pa.x, day = pd.y - pa.y, daz = pd.z - pa.z;
-    float xx, xy, xz;
+    const real4 pa = v.pos[ia], pb = v.pos[ib], pc = v.pos[ic], pd = v.pos[id];
+    const real bax = pb.x - pa.x, bay = pb.y - pa.y, baz = pb.z - pa.z;
+    const real cax = pc.x - pa.x, cay = pc.y - pa.y, caz = pc.z - pa.z;
+    const real dax = pd.x - pa.x, day = pd.y - pa.y, daz = pd.z - pa.z;
+    real xx, xy, xz;
     cross3(bax, bay, baz, cax, cay, caz, xx, xy, xz);
-    const float V = dot3(xx, xy, xz, dax, day, daz) / 6.0f;
-    const float Cv = V - V0;
-    float gbx, gby, gbz, gcx, gcy, gcz, gdx, gdy, gdz;
+    const real V = dot3(xx, xy, xz, dax, day, daz) / 6.0f;
+    const real Cv = V - V0;
+    real gbx, gby, gbz, gcx, gcy, gcz, gdx, gdy, gdz;
     cross3(cax, cay, caz, dax, day, daz, gbx, gby, gbz);
     gbx = gbx / 6.0f; gby = gby / 6.0f; gbz = gbz / 6.0f;
     cross3(dax, day, daz, bax, bay, baz, gcx, gcy, gcz);
     gcx = gcx / 6.0f; gcy = gcy / 6.0f; gcz = gcz / 6.0f;
     cross3(bax, bay, baz, cax, cay, caz, gdx, gdy, gdz);
     gdx = gdx / 6.0f; gdy = gdy / 6.0f; gdz = gdz / 6.0f;
-    const float gax = -((gbx + gcx) + gdx), gay = -((gby + gcy) + gdy), gaz = -((gbz + gcz) + gdz);
-    const float w = pa.w;
-    const float denom = w * (dot3(gax, gay, gaz, gax, gay, gaz) + dot3(gbx, gby, gbz, gbx, gby, gbz) +
+    const real gax = -((gbx + gcx) + gdx), gay = -((gby + gcy) + gdy), gaz = -((gbz + gcz) + gdz);
+    const real w = pa.w;
+    const real denom = w * (dot3(gax, gay, gaz, gax, gay, gaz) + dot3(gbx, gby, gbz, gbx, gby, gbz) +
                              dot3(gcx, gcy, gcz, gcx, gcy, gcz) + dot3(gdx, gdy, gdz, gdx, gdy, gdz));
     if (denom < 1e-12f) continue;
-    const float dl = -Cv / denom;
+    const real dl = -Cv / denom;
     const uint32_t da = v.tet_adj[ia + 1] - v.tet_adj[ia], db = v.tet_adj[ib + 1] - v.tet_adj[ib];
     const uint32_t dc = v.tet_adj[ic + 1] - v.tet_adj[ic], dd = v.tet_adj[id + 1] - v.tet_adj[id];
     const uint32_t m1 = (da < db) ? db : da, m2 = (dc < dd) ? dd : dc;
     uint32_t dm = (m1 < m2) ? m2 : m1;
     if (dm < 1u) dm = 1u;
-    const float s = 1.0f / (float)dm;
-    float gx = gax, gy = gay, gz = gaz;
+    const real s = 1.0f / (real)dm;
+    real gx = gax, gy = gay, gz = gaz;
     if ((uint32_t)i == ib) { gx = gbx; gy = gby; gz = gbz; }
     else if ((uint32_t)i == ic) { gx = gcx; gy = gcy; gz = gcz; }
     else if ((uint32_t)i == id) { gx = gdx; gy = gdy; gz = gdz; }
-    const float f = w * dl * s;
-    float c1x = gx * f, c1y = gy * f, c1z = gz * f;
-    const float cl2 = dot3(c1x, c1y, c1z, c1x, c1y, c1z);
-    const float lim = 0.5f * P->solid_radius;
+    const real f = w * dl * s;
+    real c1x = gx * f, c1y = gy * f, c1z = gz * f;
+    const real cl2 = dot3(c1x, c1y, c1z, c1x, c1y, c1z);
+    const real lim = 0.5f * P->solid_radius;
     if (cl2 > lim * lim) {
-      const float g = lim / sqrtf(cl2);
+      const real g = lim / r_sqrt(cl2);
       c1x = c1x * g; c1y = c1y * g; c1z = c1z * g;
     }
     cx = cx + c1x; cy = cy + c1y; cz = cz + c1z;
   }
-  v.delta[i] = make_float4(cx, cy, cz, 1.0f);
+  v.delta[i] = make_real4(cx, cy, cz, 1.0f);
 }
 
 // -------------------------------------------- bond update + contacts
@@ -767,36 +769,36 @@ __device__ __forceinline__ void b_solve_tets(const SimView& v, const DevParams* 
 __device__ __forceinline__ void bond_update(const SimView& v, const DevParams* __restrict__ P, int ci) {
   const uint4 c = v.cons[ci];
   if (c.w == 0u) return;
-  const float4 pa = v.pos[c.x], pb = v.pos[c.y];
-  const float ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
-  const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
-  const float rest = __uint_as_float(c.z);
+  const real4 pa = v.pos[c.x], pb = v.pos[c.y];
+  const real ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
+  const real d = r_sqrt(dot3(ex, ey, ez, ex, ey, ez));
+  const real rest = __uint_as_float(c.z);
   const bool tear = (P->tear_mode == 1) ? (d > rest * P->break_strain)
                                         : (d > rest + P->tear_gap * 2.0f * P->solid_radius);
   if (tear) {
     v.cons[ci].w = 0u;
     return;
   }
-  const float strain = (d - rest) / rest;
-  float nr = rest;
-  if (fabsf(strain) > P->plastic_threshold) nr = rest + (d - rest) * P->plastic_rate;
+  const real strain = (d - rest) / rest;
+  real nr = rest;
+  if (r_fabs(strain) > P->plastic_threshold) nr = rest + (d - rest) * P->plastic_rate;
   if (P->plastic_clamp) {
-    const float r0 = lattice_rest(v, P->spacing, c.x, c.y);
+    const real r0 = lattice_rest(v, P->spacing, c.x, c.y);
     nr = clampf(nr, 0.9f * r0, 1.25f * r0);
   }
-  if (nr != rest) v.cons[ci].z = __float_as_uint(nr);
+  if (nr != rest) v.cons[ci].z = __float_as_uint((float)nr);
 }
 
 __device__ __forceinline__ void tet_update(const SimView& v, const DevParams* __restrict__ P, int t) {
-  const float V0 = v.tet_vol[t];
+  const real V0 = v.tet_vol[t];
   if (V0 <= 0.f) return;
-  const float gap = P->tear_gap * 2.0f * P->solid_radius;
+  const real gap = P->tear_gap * 2.0f * P->solid_radius;
   for (int p = 0; p < 3; p++)
     for (int q = p + 1; q < 4; q++) {
       const uint32_t a = v.tet_idx[4 * t + p], b = v.tet_idx[4 * t + q];
-      const float4 pa = v.pos[a], pb = v.pos[b];
-      const float ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
-      const float d = sqrtf(dot3(ex, ey, ez, ex, ey, ez));
+      const real4 pa = v.pos[a], pb = v.pos[b];
+      const real ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
+      const real d = r_sqrt(dot3(ex, ey, ez, ex, ey, ez));
       if (d > lattice_rest(v, P->spacing, a, b) + gap) {
         v.tet_vol[t] = -V0;
         return;
@@ -814,35 +816,35 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   const bool walk = act && (iSolid || !P->use_mark || v.mark[i] != 0u);
   const unsigned FULL = 0xffffffffu;
   if (!__any_sync(FULL, walk)) {  // most fluid warps: nothing near a solid, no hash to compute
-    if (act && lane == 0) v.delta[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (act && lane == 0) v.delta[i] = make_real4(0.f, 0.f, 0.f, 0.f);
     return;
   }
-  float cx = 0.f, cy = 0.f, cz = 0.f, cnt = 0.f;
-  const float4 pi = walk ? v.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  real cx = 0.f, cy = 0.f, cz = 0.f, cnt = 0.f;
+  const real4 pi = walk ? v.pos[i] : make_real4(0.f, 0.f, 0.f, 0.f);
   CellHash ch;
   group_cell_hash(pi.x, pi.y, pi.z, P->inv_cell, ch);
-  const float wi = pi.w;
-  const float rs = P->solid_radius, rf = P->fluid_radius, scale = P->contact_scale;
+  const real wi = pi.w;
+  const real rs = P->solid_radius, rf = P->fluid_radius, scale = P->contact_scale;
   // a solid meets the fluid part of each bucket, a fluid particle the solid
   // part (fluid-fluid is DDR's job, solid-solid the contact cache's)
-  const float ri = iSolid ? rs : rf;
-  const float rsum = ri + (iSolid ? rf : rs);
-  const float4* __restrict__ spos = v.spos;
-  const float4* __restrict__ sfp = v.sfp;
+  const real ri = iSolid ? rs : rf;
+  const real rsum = ri + (iSolid ? rf : rs);
+  const real4* __restrict__ spos = v.spos;
+  const real4* __restrict__ sfp = v.sfp;
   auto load_fluid = [&](uint32_t e) { return sfp[e]; };  // after the displacement
   auto load_solid = [&](uint32_t e) { return spos[e]; };  // after the solve
-  auto pair = [&](uint32_t, const float4& pj) {
-    const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-    const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+  auto pair = [&](uint32_t, const real4& pj) {
+    const real ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
+    const real d2 = dot3(ex, ey, ez, ex, ey, ez);
     if (d2 >= rsum * rsum || d2 < 1e-12f) return;
-    const float wsum = wi + pj.w;
+    const real wsum = wi + pj.w;
     if (wsum == 0.f) return;
 #ifdef UPBD_PARITY_BUILD
-    const float d = sqrtf(d2);
-    const float f = (rsum - d) / d * wi / wsum * scale;
+    const real d = r_sqrt(d2);
+    const real f = (rsum - d) / d * wi / wsum * scale;
 #else
-    const float rd = rsqrtf(d2);  // d2 >= 1e-12 here
-    const float f = (rsum - d2 * rd) * rd * __fdividef(wi, wsum) * scale;
+    const real rd = r_rsqrt(d2);  // d2 >= 1e-12 here
+    const real f = (rsum - d2 * rd) * rd * r_fdiv(wi, wsum) * scale;
 #endif
     cx = cx + ex * f; cy = cy + ey * f; cz = cz + ez * f;
     cnt = cnt + 1.0f;
@@ -855,7 +857,7 @@ __device__ __forceinline__ void contacts_lane(const SimView& v, const DevParams*
   cy = lane_sum(cy);
   cz = lane_sum(cz);
   cnt = lane_sum(cnt);
-  if (act && lane == 0) v.delta[i] = make_float4(cx, cy, cz, cnt);
+  if (act && lane == 0) v.delta[i] = make_real4(cx, cy, cz, cnt);
 }
 
 // nb_pad is nb + nt rounded up to a multiple of 32, so the contact threads
@@ -877,7 +879,7 @@ __device__ __forceinline__ void b_bond_contacts(const SimView& v, const DevParam
 // -------------------------------- apply + bounds + velocity (per particle)
 // The movement allowance of xsph's list test (XSKIN above), the same float on
 // both sides of the test.
-__device__ __forceinline__ float xsph_allowance(const DevParams* __restrict__ P) {
+__device__ __forceinline__ real xsph_allowance(const DevParams* __restrict__ P) {
   return XSKIN * P->fluid_h * XMOVE_FRAC;
 }
 
@@ -888,20 +890,20 @@ __device__ __forceinline__ float xsph_allowance(const DevParams* __restrict__ P)
 // scene's SCR_XMOVE the largest distance above the recording threshold (the
 // latter one atomic per warp).
 __device__ __forceinline__ void record_move(const SimView& v, const DevParams* __restrict__ P, int i, uint32_t sl,
-                                            const float4& o, const float4& p) {
-  const float dx = p.x - o.x, dy = p.y - o.y, dz = p.z - o.z;
-  const float INF = __int_as_float(0x7f800000);
-  float m = sqrtf(dot3(dx, dy, dz, dx, dy, dz));
+                                            const real4& o, const real4& p) {
+  const real dx = p.x - o.x, dy = p.y - o.y, dz = p.z - o.z;
+  const real INF = __int_as_float(0x7f800000);
+  real m = r_sqrt(dot3(dx, dy, dz, dx, dy, dz));
   if (!(m <= 3.0e38f)) m = INF;  // NaN or inf
   const double inv = P->inv_cell;
   const bool same = floor(__dmul_rn((double)o.x, inv)) == floor(__dmul_rn((double)p.x, inv)) &&
                     floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
                     floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
-  v.smove[sl] = same ? m : INF;
+  v.smove[sl] = same ? r_to_float_up(m) : __int_as_float(0x7f800000);
   const bool rec = m > XMOVE_REC * xsph_allowance(P);
-  if (rec) atomicMax(&v.bmove[v.cell[i]], __float_as_uint(m));
+  if (rec) atomicMax(&v.bmove[v.cell[i]], __float_as_uint(r_to_float_up(m)));
   const unsigned am = __activemask();
-  const uint32_t wm = __reduce_max_sync(am, rec ? __float_as_uint(m) : 0u);
+  const uint32_t wm = __reduce_max_sync(am, rec ? __float_as_uint(r_to_float_up(m)) : 0u);
   if (wm != 0u && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&v.scratch[SCR_XMOVE], wm);
 }
 
@@ -916,17 +918,17 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
   uint32_t f = v.flags[i];
   if (!(f & F_ACTIVE)) return;
   const bool iSolid = i < v.S;
-  const float r = iSolid ? P->solid_radius : P->fluid_radius;
-  float4 p = v.pos[i];
+  const real r = iSolid ? P->solid_radius : P->fluid_radius;
+  real4 p = v.pos[i];
   const uint32_t sl = v.slot[i];
-  const float4 o = iSolid ? p : v.spos[sl];  // a fluid particle's density-pass position, read before any store
+  const real4 o = iSolid ? p : v.spos[sl];  // a fluid particle's density-pass position, read before any store
   // applyDeltaAll
   {
-    const float4 dd = v.delta[i];
-    float dx = dd.x, dy = dd.y, dz = dd.z;
-    const float m2 = dot3(dx, dy, dz, dx, dy, dz);
+    const real4 dd = v.delta[i];
+    real dx = dd.x, dy = dd.y, dz = dd.z;
+    const real m2 = dot3(dx, dy, dz, dx, dy, dz);
     if (m2 > r * r) {
-      const float g = r / sqrtf(m2);
+      const real g = r / r_sqrt(m2);
       dx = dx * g; dy = dy * g; dz = dz * g;
     }
     p.x = p.x + dx; p.y = p.y + dy; p.z = p.z + dz;
@@ -938,29 +940,29 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
     return;
   }
   // bounds
-  const float4 pv = v.prev[i];
-  float px = p.x, py = p.y, pz = p.z;
+  const real4 pv = v.prev[i];
+  real px = p.x, py = p.y, pz = p.z;
   if (py < r) {
     py = r;
-    const float mu = iSolid ? P->friction_solid : P->friction_fluid;
+    const real mu = iSolid ? P->friction_solid : P->friction_fluid;
     px = px - (px - pv.x) * mu;
     pz = pz - (pz - pv.z) * mu;
   }
   if (py < P->wall_h + r) {
-    const float lim = r + P->wall_t;
-    const float wx = P->wall_x, wz = P->wall_z;
-    if (fabsf(fabsf(px) - wx) < lim) {
-      const float side = signf(px);
-      px = (fabsf(px) < wx) ? side * (wx - lim) : side * (wx + lim);
+    const real lim = r + P->wall_t;
+    const real wx = P->wall_x, wz = P->wall_z;
+    if (r_fabs(r_fabs(px) - wx) < lim) {
+      const real side = signf(px);
+      px = (r_fabs(px) < wx) ? side * (wx - lim) : side * (wx + lim);
     }
-    if (fabsf(fabsf(pz) - wz) < lim) {
-      const float side = signf(pz);
-      pz = (fabsf(pz) < wz) ? side * (wz - lim) : side * (wz + lim);
+    if (r_fabs(r_fabs(pz) - wz) < lim) {
+      const real side = signf(pz);
+      pz = (r_fabs(pz) < wz) ? side * (wz - lim) : side * (wz + lim);
     }
   }
   bool culled = false;
   if (!iSolid) {
-    const float cr = P->cull_r;
+    const real cr = P->cull_r;
     if (py < -3.0f || px * px + pz * pz > cr * cr) {
       v.flags[i] = 0u;
       culled = true;
@@ -978,20 +980,20 @@ __device__ __forceinline__ void b_apply_bounds_vel(const SimView& v, const DevPa
     return;
   }
   // velocityUpdate
-  const float h = P->h;
-  float vx = (p.x - pv.x) / h, vy = (p.y - pv.y) / h, vz = (p.z - pv.z) / h;
-  const float damp = iSolid ? P->damp_solid : P->damp_fluid;
-  const float g = mx(0.0f, 1.0f - damp * h);
+  const real h = P->h;
+  real vx = (p.x - pv.x) / h, vy = (p.y - pv.y) / h, vz = (p.z - pv.z) / h;
+  const real damp = iSolid ? P->damp_solid : P->damp_fluid;
+  const real g = mx(0.0f, 1.0f - damp * h);
   vx = vx * g; vy = vy * g; vz = vz * g;
-  const float sp2 = dot3(vx, vy, vz, vx, vy, vz);
-  const float ms = P->max_speed;
+  const real sp2 = dot3(vx, vy, vz, vx, vy, vz);
+  const real ms = P->max_speed;
   if (sp2 > ms * ms) {
-    const float q = ms / sqrtf(sp2);
+    const real q = ms / r_sqrt(sp2);
     vx = vx * q; vy = vy * q; vz = vz * q;
   }
   if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) atomicOr(&v.scratch[SCR_HEALTH], 1u);
-  const float vw = v.vel[i].w;
-  const float4 nv = make_float4(vx, vy, vz, vw);
+  const real vw = v.vel[i].w;
+  const real4 nv = make_real4(vx, vy, vz, vw);
   v.vel[i] = nv;
   v.svel[sl] = nv;
 }
@@ -1002,24 +1004,24 @@ __device__ __forceinline__ void b_solid_visc(const SimView& v, const DevParams* 
   if (i >= v.S) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
   const uint32_t* ids = v.adj + v.S + 1;
-  float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
+  real sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
   for (uint32_t k = v.adj[i]; k < v.adj[i + 1]; k++) {
     const uint4 c = v.cons[ids[k]];
     if (c.w == 0u) continue;
     const uint32_t other = (c.x == (uint32_t)i) ? c.y : c.x;
-    const float4 vo = v.vel[other];
+    const real4 vo = v.vel[other];
     sx = sx + vo.x; sy = sy + vo.y; sz = sz + vo.z;
     m = m + 1.0f;
   }
-  const float4 vi = v.vel[i];
-  float vx = vi.x, vy = vi.y, vz = vi.z;
+  const real4 vi = v.vel[i];
+  real vx = vi.x, vy = vi.y, vz = vi.z;
   if (m > 0.f) {
-    const float mu = P->solid_viscosity;
+    const real mu = P->solid_viscosity;
     vx = vx + mu * (sx / m - vx);
     vy = vy + mu * (sy / m - vy);
     vz = vz + mu * (sz / m - vz);
   }
-  v.delta[i] = make_float4(vx, vy, vz, 0.f);
+  v.delta[i] = make_real4(vx, vy, vz, 0.f);
 }
 
 // solidViscApply, src/gpu/wgsl.js:737-742
@@ -1027,9 +1029,9 @@ __device__ __forceinline__ void b_solid_visc_apply(const SimView& v, uint32_t vb
   const int i = UPBD_VTID;
   if (i >= v.S) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
-  const float4 d = v.delta[i];
-  const float w = v.vel[i].w;
-  v.vel[i] = make_float4(d.x, d.y, d.z, w);
+  const real4 d = v.delta[i];
+  const real w = v.vel[i].w;
+  v.vel[i] = make_real4(d.x, d.y, d.z, w);
 }
 
 // xsph, src/gpu/wgsl.js:745-771 (slot-ordered groups, as b_density). The
@@ -1060,20 +1062,20 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   slot_group(v, t, myslot, i, fluid);
   const bool act = fluid && (v.flags[i] & F_ACTIVE);
   if (!__any_sync(0xffffffffu, act)) return;
-  float sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
-  const float4 pi = act ? v.spos[myslot] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const float H = P->fluid_h, H2 = H * H;
-  const float4* __restrict__ spos = v.spos;
-  const float4* __restrict__ svel = v.svel;
+  real sx = 0.f, sy = 0.f, sz = 0.f, m = 0.f;
+  const real4 pi = act ? v.spos[myslot] : make_real4(0.f, 0.f, 0.f, 0.f);
+  const real H = P->fluid_h, H2 = H * H;
+  const real4* __restrict__ spos = v.spos;
+  const real4* __restrict__ svel = v.svel;
   // position and velocity of every candidate are loaded together, before the
   // range test, and out-of-range ones add zero (the sums start at +0, so +0
   // leaves them unchanged): no load waits on the test
   struct PV {
-    float4 p, v;
+    real4 p, v;
   };
   auto load = [&](uint32_t e) { return PV{spos[e], svel[e]}; };
   auto use = [&](uint32_t e, const PV& c) {
-    const float ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
+    const real ex = c.p.x - pi.x, ey = c.p.y - pi.y, ez = c.p.z - pi.z;
     const bool in = (e != myslot) && (dot3(ex, ey, ez, ex, ey, ez) < H2);
     sx = sx + (in ? c.v.x : 0.f); sy = sy + (in ? c.v.y : 0.f); sz = sz + (in ? c.v.z : 0.f);
     m = m + (in ? 1.0f : 0.f);
@@ -1084,13 +1086,13 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   // so when it passes the buckets are not looked at (nor hashed, unless the
   // group walks).
   const uint32_t NS = (uint32_t)v.N;
-  const float allow = xsph_allowance(P), rec = XMOVE_REC * allow;
-  const float sm = act ? v.smove[myslot] : 0.f;
+  const real allow = xsph_allowance(P), rec = XMOVE_REC * allow;
+  const real sm = act ? v.smove[myslot] : 0.f;
   const uint32_t cnt = act ? v.ncount[lane * NS + myslot] : 0u;
   uint32_t over = (cnt > NL) ? 1u : 0u;
 #pragma unroll
   for (int d = 1; d < GLF; d <<= 1) over |= __shfl_xor_sync(0xffffffffu, over, d);
-  const bool quick = act && over == 0u && sm + fmaxf(rec, __uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
+  const bool quick = act && over == 0u && sm + r_fmax(rec, (real)__uint_as_float(v.scratch[SCR_XMOVE])) <= allow;
   const bool need = act && !quick;  // its buckets' movement, or the walk
   CellHash ch;
   bool listed = quick;
@@ -1108,7 +1110,7 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
 #pragma unroll
     for (int d = 1; d < GLF; d <<= 1) bm = max(bm, __shfl_xor_sync(0xffffffffu, bm, d));
     // bm holds a finite distance or +inf
-    listed = quick || (need && over == 0u && sm + fmaxf(rec, __uint_as_float(bm)) <= allow);
+    listed = quick || (need && over == 0u && sm + r_fmax(rec, (real)__uint_as_float(bm)) <= allow);
   }
   const bool walks = act && !listed;
   const bool mine = (ROLE == 0) ? act : ((ROLE == 1) ? listed : walks);
@@ -1145,18 +1147,18 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
   sz = lane_sum<GLF>(sz);
   m = lane_sum<GLF>(m);
   if (mine && lane == 0) {
-    const float4 vi = v.vel[i];
-    float vx = vi.x, vy = vi.y, vz = vi.z;
+    const real4 vi = v.vel[i];
+    real vx = vi.x, vy = vi.y, vz = vi.z;
     if (m > 0.f) {
-      const float mu = P->viscosity;
+      const real mu = P->viscosity;
       vx = vx + mu * (sx / m - vx);
       vy = vy + mu * (sy / m - vy);
       vz = vz + mu * (sz / m - vz);
     }
     if (APPLY)
-      v.vel[i] = make_float4(vx, vy, vz, 0.f);
+      v.vel[i] = make_real4(vx, vy, vz, 0.f);
     else
-      v.delta[i] = make_float4(vx, vy, vz, m);
+      v.delta[i] = make_real4(vx, vy, vz, m);
   }
 }
 

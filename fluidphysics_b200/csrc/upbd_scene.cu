@@ -160,11 +160,11 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   const bool scc = (d.features & UPBD_FEAT_SOLID_CONTACTS) != 0;
   Carver cv;
   SceneLayout L{};
-  L.pos = cv.take<float4>(v.N);
-  L.prev = cv.take<float4>(v.N);
-  L.vel = cv.take<float4>(v.N);
-  L.delta = cv.take<float4>(v.N);
-  L.dens = cv.take<float2>(v.N);
+  L.pos = cv.take<real4>(v.N);
+  L.prev = cv.take<real4>(v.N);
+  L.vel = cv.take<real4>(v.N);
+  L.delta = cv.take<real4>(v.N);
+  L.dens = cv.take<real2>(v.N);
   L.flags = cv.take<uint32_t>(v.N);
   L.cons = cv.take<uint4>(std::max(v.C, 1));
   L.adj = cv.take<uint32_t>(hs.adj.size());
@@ -179,9 +179,9 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.tvol = cv.take<float>(std::max(v.NT, 1));
   L.tadj = cv.take<uint32_t>(hs.tet_adj.size());
   L.mark = cv.take<uint32_t>(v.N);
-  L.spos = cv.take<float4>(v.N);
-  L.sdens = cv.take<float2>(v.N);
-  L.svel = cv.take<float4>(v.N);
+  L.spos = cv.take<real4>(v.N);
+  L.sdens = cv.take<real2>(v.N);
+  L.svel = cv.take<real4>(v.N);
   L.slot = cv.take<uint32_t>(v.N);
   L.fend = cv.take<uint32_t>(v.T);
   L.nbr = cv.take<uint32_t>(std::max<size_t>((size_t)v.N * GLF * NL, 1));
@@ -190,22 +190,27 @@ SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView&
   L.ascl = cv.take<float>(std::max<size_t>(hs.adj_scale.size(), 1));
   L.ccount = cv.take<uint32_t>(scc ? std::max(v.S, 1) : 1);
   L.clist = cv.take<uint32_t>(scc ? (size_t)std::max(v.S, 1) * C_K : 1);
-  L.sbuf = cv.take<float4>(2 * (size_t)std::max(v.S, 1));
-  L.sfp = cv.take<float4>(v.N);
+  L.sbuf = cv.take<real4>(2 * (size_t)std::max(v.S, 1));
+  L.sfp = cv.take<real4>(v.N);
   L.smove = cv.take<float>(v.N);
   L.bmove = cv.take<uint32_t>(v.T);
   L.scr = cv.take<uint32_t>(SCR_WORDS);
   L.par = cv.take<DevParams>(1);
+#ifdef UPBD_FP64_BUILD
+  L.conv = cv.take<float4>(v.N);
+#else
+  L.conv = 0;
+#endif
   L.bytes = cv.off;
   return L;
 }
 
 void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params) {
-  v.pos = (float4*)(base + L.pos);
-  v.prev = (float4*)(base + L.prev);
-  v.vel = (float4*)(base + L.vel);
-  v.delta = (float4*)(base + L.delta);
-  v.density = (float2*)(base + L.dens);
+  v.pos = (real4*)(base + L.pos);
+  v.prev = (real4*)(base + L.prev);
+  v.vel = (real4*)(base + L.vel);
+  v.delta = (real4*)(base + L.delta);
+  v.density = (real2*)(base + L.dens);
   v.flags = (uint32_t*)(base + L.flags);
   v.cons = (uint4*)(base + L.cons);
   v.adj = (const uint32_t*)(base + L.adj);
@@ -220,9 +225,9 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.tet_vol = (float*)(base + L.tvol);
   v.tet_adj = (const uint32_t*)(base + L.tadj);
   v.mark = (uint32_t*)(base + L.mark);
-  v.spos = (float4*)(base + L.spos);
-  v.sdens = (float2*)(base + L.sdens);
-  v.svel = (float4*)(base + L.svel);
+  v.spos = (real4*)(base + L.spos);
+  v.sdens = (real2*)(base + L.sdens);
+  v.svel = (real4*)(base + L.svel);
   v.slot = (uint32_t*)(base + L.slot);
   v.fend = (uint32_t*)(base + L.fend);
   v.nbr = (uint32_t*)(base + L.nbr);
@@ -231,13 +236,76 @@ void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params
   v.adj_scale = (const float*)(base + L.ascl);
   v.ccount = (uint32_t*)(base + L.ccount);
   v.clist = (uint32_t*)(base + L.clist);
-  v.sbuf = (float4*)(base + L.sbuf);
-  v.sfp = (float4*)(base + L.sfp);
+  v.sbuf = (real4*)(base + L.sbuf);
+  v.sfp = (real4*)(base + L.sfp);
   v.smove = (float*)(base + L.smove);
   v.bmove = (uint32_t*)(base + L.bmove);
   v.scratch = (uint32_t*)(base + L.scr);
+#ifdef UPBD_FP64_BUILD
+  v.conv = (float*)(base + L.conv);
+#endif
   if (params) *params = (DevParams*)(base + L.par);
 }
+
+#ifdef UPBD_FP64_BUILD
+namespace {
+__global__ void k_widen(double* dst, const float* src, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (double)src[i];
+}
+__global__ void k_narrow(float* dst, const double* src, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (float)src[i];
+}
+unsigned conv_blocks(size_t n) { return (unsigned)((n + 255) / 256); }
+}  // namespace
+
+cudaError_t state_to_device(real* dst, const float* src_host, size_t rows, int comps, const SimView& v,
+                            cudaStream_t st) {
+  const size_t n = rows * (size_t)comps;
+  if (n == 0) return cudaSuccess;
+  if (n > (size_t)v.N * 4) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemcpyAsync(v.conv, src_host, n * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  k_widen<<<conv_blocks(n), 256, 0, st>>>(dst, v.conv, n);
+  return cudaPeekAtLastError();
+}
+
+cudaError_t state_to_host(float* dst_host, const real* src, size_t rows, int comps, const SimView& v,
+                          cudaStream_t st) {
+  const size_t n = rows * (size_t)comps;
+  if (n == 0) return cudaSuccess;
+  if (n > (size_t)v.N * 4) return cudaErrorInvalidValue;
+  k_narrow<<<conv_blocks(n), 256, 0, st>>>(v.conv, src, n);
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(dst_host, v.conv, n * sizeof(float), cudaMemcpyDeviceToHost, st);
+}
+
+cudaError_t state_to_f32(float* dst_dev, const real* src, size_t rows, int comps, cudaStream_t st) {
+  const size_t n = rows * (size_t)comps;
+  if (n == 0) return cudaSuccess;
+  k_narrow<<<conv_blocks(n), 256, 0, st>>>(dst_dev, src, n);
+  return cudaPeekAtLastError();
+}
+#else
+cudaError_t state_to_device(real* dst, const float* src_host, size_t rows, int comps, const SimView&,
+                            cudaStream_t st) {
+  const size_t bytes = rows * (size_t)comps * sizeof(float);
+  return bytes ? cudaMemcpyAsync(dst, src_host, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+}
+
+cudaError_t state_to_host(float* dst_host, const real* src, size_t rows, int comps, const SimView&,
+                          cudaStream_t st) {
+  const size_t bytes = rows * (size_t)comps * sizeof(float);
+  return bytes ? cudaMemcpyAsync(dst_host, src, bytes, cudaMemcpyDeviceToHost, st) : cudaSuccess;
+}
+
+cudaError_t state_to_f32(float* dst_dev, const real* src, size_t rows, int comps, cudaStream_t st) {
+  const size_t bytes = rows * (size_t)comps * sizeof(float);
+  return bytes ? cudaMemcpyAsync(dst_dev, src, bytes, cudaMemcpyDeviceToDevice, st) : cudaSuccess;
+}
+#endif
 
 cudaError_t upload_scene(const HostScene& hs, const SimView& v, cudaStream_t st) {
   cudaError_t e = cudaMemcpyAsync((void*)v.adj, hs.adj.data(), hs.adj.size() * 4, cudaMemcpyHostToDevice, st);
@@ -249,10 +317,8 @@ cudaError_t upload_scene(const HostScene& hs, const SimView& v, cudaStream_t st)
     e = cudaMemcpyAsync((void*)v.tet_adj, hs.tet_adj.data(), hs.tet_adj.size() * 4, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && !hs.tet_idx.empty())
     e = cudaMemcpyAsync(v.tet_idx, hs.tet_idx.data(), hs.tet_idx.size() * 4, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(v.pos, hs.pos.data(), hs.pos.size() * 16, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(v.prev, hs.pos.data(), hs.pos.size() * 16, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = state_to_device((real*)v.pos, (const float*)hs.pos.data(), hs.pos.size(), 4, v, st);
+  if (e == cudaSuccess) e = state_to_device((real*)v.prev, (const float*)hs.pos.data(), hs.pos.size(), 4, v, st);
   if (e == cudaSuccess && v.C > 0)
     e = cudaMemcpyAsync(v.cons, hs.cons.data(), (size_t)v.C * 16, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && v.NT > 0)
@@ -342,11 +408,14 @@ cudaError_t upload_prepared(const PreparedScene& ps, const SimView& v, cudaStrea
   if (e == cudaSuccess) e = up(v.tet_idx, L.tet_idx.data(), L.tet_idx.size() * 4);
   if (e == cudaSuccess) e = up(v.cons, L.cons.data(), L.cons.size() * 16);
   if (e == cudaSuccess) e = up(v.tet_vol, L.tet_vol.data(), L.tet_vol.size() * 4);
-  if (e == cudaSuccess) e = up(v.pos, L.pos.data(), (size_t)S * 16);
-  if (e == cudaSuccess) e = up(v.prev, L.pos.data(), (size_t)S * 16);
-  if (e == cudaSuccess) e = up(v.pos + S, ps.fluid_pos.data(), ps.fluid_pos.size() * 16);
-  if (e == cudaSuccess) e = up(v.prev + S, ps.fluid_prev.data(), ps.fluid_prev.size() * 16);
-  if (e == cudaSuccess) e = up(v.vel + S, ps.fluid_vel.data(), ps.fluid_vel.size() * 16);
+  auto rows = [&](real4* dst, const std::vector<float4>& src, size_t n) {
+    return n ? state_to_device((real*)dst, (const float*)src.data(), n, 4, v, st) : cudaSuccess;
+  };
+  if (e == cudaSuccess) e = rows(v.pos, L.pos, (size_t)S);
+  if (e == cudaSuccess) e = rows(v.prev, L.pos, (size_t)S);
+  if (e == cudaSuccess) e = rows(v.pos + S, ps.fluid_pos, ps.fluid_pos.size());
+  if (e == cudaSuccess) e = rows(v.prev + S, ps.fluid_prev, ps.fluid_prev.size());
+  if (e == cudaSuccess) e = rows(v.vel + S, ps.fluid_vel, ps.fluid_vel.size());
   if (e == cudaSuccess && S + ps.n_fluid > 0) {
     // solids and placed fluid active (a pageable copy: staged before return)
     std::vector<uint32_t> f((size_t)S + ps.n_fluid, F_ACTIVE);

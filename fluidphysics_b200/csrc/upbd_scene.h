@@ -34,7 +34,7 @@ void build_scene(const upbd_scene_desc& d, HostScene& out);
 struct SceneLayout {
   size_t pos, prev, vel, delta, dens, flags, cons, adj, counts, start, entries, tmp, ticket, cell, tiles;
   size_t tidx, tvol, tadj, mark, spos, sdens, svel, slot, fend, nbr, ncount, aoth, ascl, ccount, clist;
-  size_t sbuf, sfp, smove, bmove, scr, par;
+  size_t sbuf, sfp, smove, bmove, scr, par, conv;
   size_t bytes;
 };
 
@@ -44,6 +44,18 @@ struct SceneLayout {
 // into an arena that starts at base.
 SceneLayout layout_scene(const upbd_scene_desc& d, const HostScene& hs, SimView& v);
 void bind_scene(const SceneLayout& L, char* base, SimView& v, DevParams** params);
+
+// Copies of particle-state rows (comps = 4 for pos/prev/vel/delta, 2 for
+// density) between host float rows and device rows of the scalar type
+// `real`, asynchronous on st. In the FP32 builds they are plain copies; in
+// the FP64 build the rows pass through v.conv and a conversion kernel (so
+// calls on one stream must not overlap the caller's use of v.conv).
+// state_to_f32 writes float rows to device memory (the readback staging).
+cudaError_t state_to_device(real* dst, const float* src_host, size_t rows, int comps, const SimView& v,
+                            cudaStream_t st);
+cudaError_t state_to_host(float* dst_host, const real* src, size_t rows, int comps, const SimView& v,
+                          cudaStream_t st);
+cudaError_t state_to_f32(float* dst_dev, const real* src, size_t rows, int comps, cudaStream_t st);
 
 // Uploads into a zeroed arena: the static CSR data and tets, then the
 // initial state of GpuSim's constructor and resetSolid (src/gpu/sim.js:174,

@@ -281,6 +281,34 @@ def test_substeps_within_tolerance_product_build(which, request):
     print(which, errs)
 
 
+@pytest.mark.parametrize("which", ["c1_settled", "c2_settled"])
+def test_fp64_build_substeps_match_fp64_oracle(which, request):
+    """The test-only FP64 build (the same pass bodies on double) against the
+    oracle in double, one substep at a time from identical states: within
+    1e-7 of the basin extent in position and 1e-6 of maxSpeed in velocity,
+    a hundred times inside the FP32 product build's bounds (what remains is
+    the float uniforms and constants and the float rounding of the readback)."""
+    sc, st, cons = request.getfixturevalue(which)
+    sim = sim_from_scene(sc, "fp64")
+    load_state(sim, st, cons)
+    o2 = o2_from_scene(sc, 1)
+    o2.write_state(**st)
+    o2.write_constraints(cons)
+    h = sc.dt / sc.substeps
+    for k in range(2):
+        sim.substep_partial(h, 1000)
+        o2.substep_partial(h, 1000)
+        r = o2.read_state()
+        assert_states_close(sim.read_state(), r, f"fp64 substep {k}", pos_rtol=1e-7, vel_rtol=1e-6)
+        # the next substep again from one state (the oracle's, rounded to the
+        # float rows both sides load)
+        r = {key: (val.astype(np.float32) if val.dtype == np.float64 else val) for key, val in r.items()}
+        c = o2.read_constraints()[0]
+        load_state(sim, r, c)
+        o2.write_state(**r)
+        o2.write_constraints(c)
+
+
 def test_frame_parity_build_bit_exact(c1_settled):
     sc, st, cons = c1_settled
     sim = sim_from_scene(sc, "parity")
