@@ -54,6 +54,9 @@ def load():
         "o2_write_constraints": (None, [P, U]), "o2_read_adjacency": (None, [P, U]),
         "o2_read_grid": (None, [P, U, U, U]), "o2_read_tets": (None, [P, U]),
         "o2_read_tet_adjacency": (None, [P, U]),
+        "o2_run_pass_x": (I, [P, I, C.c_double, F]), "o2_write_delta": (None, [P, D]),
+        "o2_read_contact_cache": (None, [P, U, U]), "o2_write_contact_cache": (None, [P, U, U]),
+        "o2_write_tets": (None, [P, U]),
         "o2_emit": (None, [P, I, F, F, F, F, C.c_float, C.c_float]),
         "o2_emit_particles": (None, [P, I, F, F, C.c_double]),
         "o2_slice_now": (C.c_uint32, [P, D, D, D]), "o2_slice": (None, [P, D, D, D]),
@@ -246,6 +249,38 @@ class O2:
     def write_constraints(self, cons) -> None:
         c = np.ascontiguousarray(cons, dtype=np.uint32)
         self.lib.o2_write_constraints(self.h, c.ctypes.data_as(C.POINTER(C.c_uint32)))
+
+    # single passes outside o2_run_pass's set (the oracle's own ids)
+    PASS_X = dict(INTEGRATE=101, COLLECT=102, SOLID_SOLVE=103, APPLY_SOLID=104, SOLVE_TETS=105,
+                  APPLY_SOLID_CONTACTS=106, SOLID_CONTACTS=107, BOND_UPDATE=108, TET_UPDATE=109,
+                  SOLID_VISC=110, SOLID_VISC_APPLY=111, EMIT=112)
+
+    def run_pass_x(self, name: str, h: float, grab_delta_sub=None) -> None:
+        g = None if grab_delta_sub is None else (C.c_float * 3)(*[float(x) for x in grab_delta_sub])
+        if self.lib.o2_run_pass_x(self.h, self.PASS_X[name], h, g) != 0:
+            raise ValueError(f"pass {name} cannot run alone")
+
+    def write_delta(self, d4) -> None:
+        d = np.ascontiguousarray(d4, dtype=np.float64)
+        self.lib.o2_write_delta(self.h, d.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def read_contact_cache(self):
+        S = self.info.solid_n
+        cc = np.empty(S, np.uint32)
+        cl = np.empty(S * 40, np.uint32)
+        self.lib.o2_read_contact_cache(self.h, cc.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                       cl.ctypes.data_as(C.POINTER(C.c_uint32)))
+        return cc, cl
+
+    def write_contact_cache(self, ccount, clist) -> None:
+        cc = np.ascontiguousarray(ccount, dtype=np.uint32)
+        cl = np.ascontiguousarray(clist, dtype=np.uint32)
+        self.lib.o2_write_contact_cache(self.h, cc.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                        cl.ctypes.data_as(C.POINTER(C.c_uint32)))
+
+    def write_tets(self, tets5) -> None:
+        t = np.ascontiguousarray(tets5, dtype=np.uint32)
+        self.lib.o2_write_tets(self.h, t.ctypes.data_as(C.POINTER(C.c_uint32)))
 
     def read_adjacency(self) -> np.ndarray:
         a = np.empty(self.info.solid_n + 1 + 2 * self.info.num_cons, np.uint32)

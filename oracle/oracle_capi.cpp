@@ -220,6 +220,70 @@ int o2_run_pass(void* h, int pass, double hh) {
 }
 void o2_set_iters(void* h, int iters) { DISPATCH(h, S_.iters = iters); }
 
+// Single passes of the WGSL schedule that o2_run_pass does not cover (ids
+// private to the oracle, for the per-pass comparison with the reference's
+// kernels run by tests/golden/wgslmini.py).
+enum {
+  O2X_INTEGRATE = 101, O2X_COLLECT, O2X_SOLID_SOLVE, O2X_APPLY_SOLID, O2X_SOLVE_TETS,
+  O2X_APPLY_SOLID_CONTACTS, O2X_SOLID_CONTACTS, O2X_BOND_UPDATE, O2X_TET_UPDATE, O2X_SOLID_VISC,
+  O2X_SOLID_VISC_APPLY, O2X_EMIT
+};
+int o2_run_pass_x(void* h, int pass, double hh, const float* grab_delta_sub) {
+  int rc = 0;
+  DISPATCH(h, {
+    using R = decltype(S_.P.h);
+    S_.P.h = (R)hh;
+    if (grab_delta_sub) S_.grabDeltaSub = {(R)grab_delta_sub[0], (R)grab_delta_sub[1], (R)grab_delta_sub[2]};
+    switch (pass) {
+      case O2X_INTEGRATE: S_.passIntegrate(); break;
+      case O2X_COLLECT: S_.passCollectContacts(); break;
+      case O2X_SOLID_SOLVE: S_.passSolidSolve(); break;
+      case O2X_APPLY_SOLID: S_.passApplySolid(); break;
+      case O2X_SOLVE_TETS: S_.passSolveTets(); break;
+      case O2X_APPLY_SOLID_CONTACTS: S_.passApplySolidContacts(); break;
+      case O2X_SOLID_CONTACTS: S_.passSolidContacts(); break;
+      case O2X_BOND_UPDATE: S_.passBondUpdate(); break;
+      case O2X_TET_UPDATE: S_.passTetUpdate(); break;
+      case O2X_SOLID_VISC: S_.passSolidVisc(); break;
+      case O2X_SOLID_VISC_APPLY: S_.passSolidViscApply(); break;
+      case O2X_EMIT: S_.passEmit(); break;
+      default: rc = -1;
+    }
+  });
+  return rc;
+}
+void o2_write_delta(void* h, const double* d4) {
+  DISPATCH(h, {
+    using R = decltype(S_.P.h);
+    for (int i = 0; i < S_.N; i++) S_.delta[i] = {(R)d4[4*i], (R)d4[4*i+1], (R)d4[4*i+2], (R)d4[4*i+3]};
+  });
+}
+// the solid contact cache: ccount[S] and clist[S * C_K]
+void o2_read_contact_cache(void* h, uint32_t* ccount, uint32_t* clist) {
+  DISPATCH(h, {
+    std::memcpy(ccount, S_.ccount.data(), S_.ccount.size() * 4);
+    std::memcpy(clist, S_.clist.data(), S_.clist.size() * 4);
+  });
+}
+void o2_write_contact_cache(void* h, const uint32_t* ccount, const uint32_t* clist) {
+  DISPATCH(h, {
+    std::memcpy(S_.ccount.data(), ccount, S_.ccount.size() * 4);
+    std::memcpy(S_.clist.data(), clist, S_.clist.size() * 4);
+  });
+}
+// tets as the reference packs them: [a, b, c, d, rest volume f32 bits] each
+void o2_write_tets(void* h, const uint32_t* tets5) {
+  DISPATCH(h, {
+    using R = decltype(S_.P.h);
+    for (int t = 0; t < S_.NT; t++) {
+      for (int q = 0; q < 4; q++) S_.tetIdx[4*t+q] = tets5[5*t+q];
+      float v;
+      std::memcpy(&v, &tets5[5*t+4], 4);
+      S_.tetVol[t] = (R)v;
+    }
+  });
+}
+
 void o2_read_state(void* h, double* pos4, double* prev4, double* vel4, double* dens2,
                    uint32_t* flags) {
   DISPATCH(h, {

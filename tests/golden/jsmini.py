@@ -57,6 +57,28 @@ def to_number(v):
     return math.nan
 
 
+def js_to_string(v) -> str:
+    """ToString of a primitive (template substitutions)."""
+    if v is True:
+        return "true"
+    if v is False:
+        return "false"
+    if v is None:
+        return "null"
+    if v is UNDEF:
+        return "undefined"
+    if isinstance(v, (int, float)) and not isinstance(v, bool):
+        f = float(v)
+        if math.isnan(f):
+            return "NaN"
+        if math.isinf(f):
+            return "Infinity" if f > 0 else "-Infinity"
+        if f == int(f) and abs(f) < 1e21:
+            return str(int(f))
+        return repr(f)
+    return str(v)
+
+
 def to_int32(v) -> int:
     x = to_number(v)
     if not math.isfinite(x):
@@ -257,11 +279,60 @@ class Tok:
         return f"{self.kind}:{self.val}"
 
 
+_TPL_ESC = {"n": "\n", "t": "\t", "r": "\r", "\\": "\\", "`": "`", "$": "$", "'": "'", '"': '"', "0": "\0"}
+
+
+def _lex_template(src: str, i: int):
+    """A template literal starting at the backtick src[i]: returns (cooked
+    text parts, substitution sources, index after the closing backtick)."""
+    j = i + 1
+    parts, subs, buf = [], [], []
+    while True:
+        if j >= len(src):
+            raise SyntaxError("unterminated template literal")
+        c = src[j]
+        if c == "\\":
+            nxt = src[j + 1]
+            buf.append(_TPL_ESC.get(nxt, nxt))
+            j += 2
+            continue
+        if c == "`":
+            break
+        if c == "$" and src[j + 1:j + 2] == "{":
+            parts.append("".join(buf))
+            buf = []
+            depth, k = 1, j + 2
+            while depth:
+                ch = src[k]
+                if ch in "'\"":  # a quoted string inside the substitution
+                    k += 1
+                    while src[k] != ch:
+                        k += 2 if src[k] == "\\" else 1
+                elif ch == "{":
+                    depth += 1
+                elif ch == "}":
+                    depth -= 1
+                k += 1
+            subs.append(src[j + 2:k - 1])
+            j = k
+            continue
+        buf.append(c)
+        j += 1
+    parts.append("".join(buf))
+    return parts, subs, j + 1
+
+
 def lex(src: str) -> list[Tok]:
     out = []
     nl = False
     i = 0
     while i < len(src):
+        if src[i] == "`":
+            parts, subs, i2 = _lex_template(src, i)
+            out.append(Tok("tpl", (parts, [lex(x) for x in subs]), nl, i))
+            nl = False
+            i = i2
+            continue
         m = TOKEN_RE.match(src, i)
         if not m:
             raise SyntaxError(f"bad char {src[i]!r} at {i}")
@@ -692,6 +763,9 @@ class Parser:
             return ("num", tok.val)
         if tok.kind == "str":
             return ("str", tok.val)
+        if tok.kind == "tpl":
+            parts, subs = tok.val
+            return ("tpl", tuple(parts), tuple(Parser(t).expression() for t in subs))
         if tok.kind == "id":
             v = tok.val
             if v == "this":
@@ -1172,6 +1246,19 @@ class Compiler:
     def e_lit(self, n):
         v = n[1]
         return lambda env: v
+
+    def e_tpl(self, n):
+        # template literal: the text parts with each substitution's ToString
+        parts = n[1]
+        subs = [self.expr(x) for x in n[2]]
+
+        def f(env):
+            out = [parts[0]]
+            for k, g in enumerate(subs):
+                out.append(js_to_string(g(env)))
+                out.append(parts[k + 1])
+            return "".join(out)
+        return f
 
     def e_this(self, n):
         def f(env):
