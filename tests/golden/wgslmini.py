@@ -40,8 +40,6 @@ import warnings
 
 import numpy as np
 
-warnings.filterwarnings("ignore", category=RuntimeWarning)
-
 F32, I32, U32, BOOL = np.float32, np.int32, np.uint32, np.bool_
 
 # ---------------------------------------------------------------- lexer
@@ -820,6 +818,12 @@ class Module:
     def dispatch(self, entry: str, workgroups: int) -> None:
         """dispatchWorkgroups(workgroups) of an entry point: invocations in
         global-id order."""
+        with warnings.catch_warnings(), np.errstate(all="ignore"):
+            # u32 / i32 arithmetic wraps and f32 may overflow to inf, as in WGSL
+            warnings.simplefilter("ignore", RuntimeWarning)
+            self._dispatch(entry, workgroups)
+
+    def _dispatch(self, entry: str, workgroups: int) -> None:
         fn = self.fns[entry]
         size = int(fn[5]["workgroup_size"][0])
         body = self._function(entry)
