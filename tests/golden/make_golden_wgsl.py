@@ -26,7 +26,9 @@ frame 4) so that fluid, bodies, the floor and the cut faces are in contact:
            cap, the slip), grabRelease;
   emit     the hose emit kernel (96 particles);
   tools    cut + cutTets with a wedge through the body, pick on five rays,
-           countActive.
+           countActive;
+  frame    one whole frame: a 32-particle emit, five substeps, a queued cut
+           and the active count (only the end state is kept).
 
 For every pass the file keeps the buffers the pass changed, so a test can
 rebuild the state before each pass and compare the oracle's pass on it.
@@ -192,6 +194,47 @@ class Recorder:
         self.run("gridScatter", C["TOTAL"], uniform)
 
 
+def substep(r, C: dict, u: dict, iters: int) -> None:
+    """One substep in GpuSim.encode's pass order (src/gpu/sim.js:352-385)."""
+    S_, F, N = C["SOLID_N"], C["MAX_FLUID"], C["TOTAL"]
+    r.run("integrate", N, u)
+    r.grid(C, u)
+    for k in ("fluidDensity", "fluidDisp", "applyDeltaFluid"):
+        r.run(k, F, u)
+    r.run("collectContacts", S_, u)
+    for it in range(iters):
+        r.run("solidSolve", S_, u)
+        r.run("applyDeltaSolid", S_, u)
+        r.run("solveTets", S_, u)
+        r.run("applySolidContacts", S_, u)
+        r.run("solidContacts", S_, u)
+        r.run("applySolidContacts", S_, u)
+    r.run("bondUpdate", C["NUM_CONS"], u)
+    r.run("tetUpdate", C["NUM_TETS"], u)
+    for k in ("contacts", "applyDeltaAll", "bounds", "velocityUpdate"):
+        r.run(k, N, u)
+    if u["solidViscosity"] > 0:
+        r.run("solidVisc", S_, u)
+        r.run("solidViscApply", S_, u)
+    r.run("xsph", F, u)
+    r.run("xsphApply", F, u)
+
+
+class Runner(Recorder):
+    """Runs passes without recording them (whole frames: only the end state
+    is kept)."""
+
+    def __init__(self, mod: W.Module, bufs: dict):
+        self.m, self.b = mod, bufs
+        for k, v in bufs.items():
+            mod.bind(k, v)
+        self.meta, self.tag, self.out = [], "", {}
+
+    def run(self, kernel: str, n_invocations: int, uniform: dict, wg_size: int = 256, label: str | None = None):
+        self.m.set_uniform("P", uniform)
+        self.m.dispatch(kernel, max(1, math.ceil(n_invocations / wg_size)))
+
+
 def main():
     ref = reference_dir()
     sc = golden_scene()
@@ -207,26 +250,7 @@ def main():
     print("substep", flush=True)
     m = W.Module(src)
     r = Recorder(m, buffers(o2, C), "substep", out, meta)
-    r.run("integrate", N, base)
-    r.grid(C, base)
-    for k in ("fluidDensity", "fluidDisp", "applyDeltaFluid"):
-        r.run(k, F, base)
-    r.run("collectContacts", S_, base)
-    for it in range(iters):
-        r.run("solidSolve", S_, base)
-        r.run("applyDeltaSolid", S_, base)
-        r.run("solveTets", S_, base)
-        r.run("applySolidContacts", S_, base)
-        r.run("solidContacts", S_, base)
-        r.run("applySolidContacts", S_, base)
-    r.run("bondUpdate", NC, base)
-    r.run("tetUpdate", NT, base)
-    for k in ("contacts", "applyDeltaAll", "bounds", "velocityUpdate"):
-        r.run(k, N, base)
-    r.run("solidVisc", S_, base)
-    r.run("solidViscApply", S_, base)
-    r.run("xsph", F, base)
-    r.run("xsphApply", F, base)
+    substep(r, C, base, iters)
 
     # ---- bond and tet rules on a stretched state
     print("bonds", flush=True)
@@ -304,6 +328,29 @@ def main():
         b["gridA"][C["TABLE"] * 2 + N] = 0xFFFFFFFF  # S_PICK reset, as GpuSim.pick does before dispatching
         r.run("pick", S_, uniforms(sc, pickO=[*ro, 0.3], pickD=[*rd, 0.0]), label=f"pick {k}")
     r.run("countActive", F, base)
+
+    # ---- one whole frame: emit, the substeps, the queued cut, the active count
+    # (GpuSim.encode, src/gpu/sim.js:333-392)
+    print("frame", flush=True)
+    b = buffers(o2, C)
+    for k in MUTABLE:
+        out[f"frame/start/{k}"] = b[k].copy()
+    r = Runner(W.Module(src), b)
+    emit_u = dict(emitCount=32, emitStart=int(o2.info.fluid_next), emitPos=[-0.15, 1.5, 0.2, 2.5],
+                  emitDir=[0.0, -1.0, 0.0, 0.3], emitSide=[1.0, 0.0, 0.0, 0.0], emitUp=[0.0, 0.0, 1.0, 0.0])
+    ow, d1w, d2w = S.wedge_through(sc.desc.cube_center, 31)
+    frame_u = uniforms(sc, cutO=[*ow, 0.0], cutD1=[*d1w, 0.0], cutD2=[*d2w, 0.0], **emit_u)
+    r.run("emit", 32, frame_u, wg_size=64)
+    for k in range(sc.substeps):
+        substep(r, C, frame_u, iters)
+    r.run("cut", NC, frame_u)
+    r.run("cutTets", NT, frame_u)
+    r.run("countActive", F, frame_u)
+    for k in MUTABLE:
+        out[f"frame/end/{k}"] = b[k].copy()
+    meta.append({"scenario": "frame", "index": 0, "kernel": "frame", "label": "frame", "changed": [],
+                 "uniform": {u: (list(map(float, v)) if isinstance(v, list) else float(v)) for u, v in frame_u.items()},
+                 "wedge": [list(map(float, ow)), list(map(float, d1w)), list(map(float, d2w))]})
 
     out["meta"] = np.frombuffer(json.dumps({"C": C, "passes": meta}).encode(), dtype=np.uint8)
     np.savez_compressed(OUT, **out)
