@@ -223,7 +223,8 @@ class UpbdError(RuntimeError):
         self.code = code
 
 
-LIB_NAMES = {"product": "libupbd.so", "parity": "libupbd_parity.so", "fp64": "libupbd_fp64.so"}
+LIB_NAMES = {"product": "libupbd.so", "parity": "libupbd_parity.so", "fp64": "libupbd_fp64.so",
+             "checked": "libupbd_checked.so"}
 
 
 def lib_path(variant: str = "product") -> Path:
@@ -231,9 +232,10 @@ def lib_path(variant: str = "product") -> Path:
 
 
 def load(variant: str = "product") -> C.CDLL:
-    """Load libupbd.so ("product"), libupbd_parity.so ("parity") or the
-    test-only libupbd_fp64.so ("fp64": the same pass bodies on double, the
-    single-scene entry points only)."""
+    """Load libupbd.so ("product"), libupbd_parity.so ("parity") or one of
+    the test-only builds: libupbd_fp64.so ("fp64": the same pass bodies on
+    double, the single-scene entry points only) and libupbd_checked.so
+    ("checked": the product with device-side index guards)."""
     if variant in _libs:
         return _libs[variant]
     path = lib_path(variant)

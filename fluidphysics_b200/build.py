@@ -5,6 +5,9 @@ Outputs (next to this file):
   libupbd_parity.so  the same sources with --fmad=false, so every FP32
                      operation rounds exactly as the CPU oracle's does
                      (per-pass bit-exact parity checks)
+  libupbd_checked.so test-only: the product sources with device-side index
+                     guards (UPBD_CHECKED_BUILD): an out-of-range index sets a
+                     health bit and its access is skipped
   libupbd_fp64.so    test-only: the single-scene library with the pass
                      bodies instantiated on double (UPBD_FP64_BUILD), the
                      reference trajectory of the 600-frame drift test
@@ -31,6 +34,7 @@ TARGETS = {
     "libupbd.so": SOURCES,
     "libupbd_parity.so": SOURCES,
     "libupbd_fp64.so": ["upbd.cu", "upbd_scene.cu"],
+    "libupbd_checked.so": SOURCES,
 }
 
 
@@ -66,6 +70,8 @@ def build(force: bool = False, verbose: bool = False) -> list[Path]:
             flags += ["--fmad=false", "-DUPBD_PARITY_BUILD=1"]
         if name == "libupbd_fp64.so":
             flags += ["-DUPBD_FP64_BUILD=1"]
+        if name == "libupbd_checked.so":
+            flags += ["-DUPBD_CHECKED_BUILD=1"]
         cmd = [nvcc, *ARCH, *flags, "-o", str(out) + ".tmp", *[str(CSRC / s) for s in srcs]]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

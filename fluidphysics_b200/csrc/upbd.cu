@@ -682,6 +682,8 @@ int upbd_sync(upbd_sim* s) {
   const uint32_t hb = ((volatile uint32_t*)s->hmapped)[HM_HEALTH];
   if (hb & UPBD_HEALTH_TIMEOUT) return fail(s, UPBD_ERR_TIMEOUT, "a bounded device wait gave up");
   if (hb & UPBD_HEALTH_NAN) return fail(s, UPBD_ERR_NAN, "non-finite velocity detected");
+  if (hb & UPBD_HEALTH_BOUNDS)
+    return fail(s, UPBD_ERR_INTERNAL, "an index out of range was skipped (checked build)");
   return UPBD_OK;
 }
 

@@ -769,6 +769,9 @@ int upbd_batch_sync(upbd_batch* b) {
     const uint32_t hb = ((volatile uint32_t*)b->hmapped)[(size_t)kv.second.hm_slot * HM_WORDS + HM_HEALTH];
     if (hb & UPBD_HEALTH_NAN)
       return bfail(b, UPBD_ERR_NAN, "non-finite velocity detected in scene " + std::to_string(kv.first));
+    if (hb & UPBD_HEALTH_BOUNDS)
+      return bfail(b, UPBD_ERR_INTERNAL,
+                   "an index out of range was skipped in scene " + std::to_string(kv.first) + " (checked build)");
   }
   return UPBD_OK;
 }

@@ -205,6 +205,25 @@ struct CellHash {
   }
 };
 
+// Index guard of the checked build (UPBD_CHECKED_BUILD, libupbd_checked.so):
+// the indices the gathers read from device arrays (bucket members, list
+// entries, CSR constraint ids and other endpoints, bucket slots, tet
+// corners, contact-cache entries) are tested against their array's extent
+// before use; an index out of range sets UPBD_HEALTH_BOUNDS in the scene's
+// health word (upbd_health, upbd_sync) and its access is skipped instead of
+// faulting. In the product and parity builds the guard is the constant true
+// and generates no code.
+#ifdef UPBD_CHECKED_BUILD
+__device__ __forceinline__ bool idx_ok(uint32_t* scratch, uint64_t idx, uint64_t n) {
+  if (idx < n) return true;
+  if (scratch) atomicOr(&scratch[SCR_HEALTH], 8u);  // UPBD_HEALTH_BOUNDS (the stateless grid build has none)
+  return false;
+}
+#define UPBD_IDX_OK(v, idx, n) (::upbd::idx_ok((v).scratch, (uint64_t)(idx), (uint64_t)(n)))
+#else
+#define UPBD_IDX_OK(v, idx, n) (true)
+#endif
+
 // Neighbour gathers run G lanes per particle (lane_strided below deals the
 // candidates to the lanes); each lane accumulates its own partial sums from
 // zero and the G partials are combined by a fixed xor butterfly, so the
@@ -352,7 +371,7 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
         base = s_base[g][k];
       }
       const uint32_t e = base + c;
-      use(e, load(e));
+      if (UPBD_IDX_OK(v, e, v.N)) use(e, load(e));
     }
   } else {
     // U candidates per step, their loads in flight together (for the few
@@ -369,6 +388,7 @@ __device__ __forceinline__ void lane_strided(const SimView& v, const CellHash& c
             base = s_base[g][k];
           }
           e[u] = base + c;
+          if (!UPBD_IDX_OK(v, e[u], v.N)) e[u] = 0u;  // out of range: slot 0 instead (reported)
         } else {
           e[u] = e[0];  // c0 < run: a valid slot, loaded again and not used
         }
@@ -418,7 +438,8 @@ __device__ __forceinline__ void lane_staged(const SimView& v, const CellHash& ch
           next = s_off[gw][k + 1];
           base = s_base[gw][k];
         }
-        const uint32_t e = base + c;
+        uint32_t e = base + c;
+        if (!UPBD_IDX_OK(v, e, v.N)) e = 0u;  // out of range: slot 0 instead (reported)
         s_e[w][L] = e;
         s_x[w][L] = load(e);
       }

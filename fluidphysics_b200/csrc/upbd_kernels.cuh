@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(256) k_cut(SimView v, const DevParams* __restr
   const double nz = __dsub_rn(__dmul_rn(d1x, d2y), __dmul_rn(d1y, d2x));
   const double nl = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(nx, nx), __dmul_rn(ny, ny)), __dmul_rn(nz, nz)));
   if (nl < 1e-8) return;
+  if (!UPBD_IDX_OK(v, cc.x, v.S) || !UPBD_IDX_OK(v, cc.y, v.S)) return;
   const real4 A = v.pos[cc.x], B = v.pos[cc.y];
   const double ax = A.x, ay = A.y, az = A.z, bx = B.x, by = B.y, bz = B.z;
   const double sa = __dadd_rn(__dadd_rn(__dmul_rn(__dsub_rn(ax, ox), nx), __dmul_rn(__dsub_rn(ay, oy), ny)),
@@ -164,8 +165,10 @@ __global__ void __launch_bounds__(256) k_cut_tets(SimView v, const DevParams* __
   if (dot3(nx, ny, nz, nx, ny, nz) < 1e-16f) return;
   for (int p = 0; p < 3; p++)
     for (int q = p + 1; q < 4; q++) {
-      const real4 A = v.pos[v.tet_idx[4 * t + p]];
-      const real4 B = v.pos[v.tet_idx[4 * t + q]];
+      const uint32_t ta = v.tet_idx[4 * t + p], tb = v.tet_idx[4 * t + q];
+      if (!UPBD_IDX_OK(v, ta, v.S) || !UPBD_IDX_OK(v, tb, v.S)) return;
+      const real4 A = v.pos[ta];
+      const real4 B = v.pos[tb];
       const real pax = A.x - ox, pay = A.y - oy, paz = A.z - oz;
       const real pbx = B.x - ox, pby = B.y - oy, pbz = B.z - oz;
       const real sa = dot3(pax, pay, paz, nx, ny, nz);

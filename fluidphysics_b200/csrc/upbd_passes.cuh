@@ -184,7 +184,8 @@ __device__ __forceinline__ void b_scatter(const SimView& v, uint32_t vb) {
   if (i >= v.N) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
   const uint32_t h = v.cell[i];
-  v.tmp[v.start[h] + v.ticket[i]] = (uint32_t)i;
+  const uint32_t at = v.start[h] + v.ticket[i];
+  if (UPBD_IDX_OK(v, at, v.N)) v.tmp[at] = (uint32_t)i;
 }
 
 // Deterministic membership: particle i goes to start[h] + #{j in bucket : j > i},
@@ -197,11 +198,13 @@ __device__ __forceinline__ void b_rankfix(const SimView& v, uint32_t vb) {
   const uint32_t h = v.cell[i];
   const uint32_t s = v.start[h], e = v.start[h + 1];
   uint32_t rank = 0, solids = 0;
+  if (!UPBD_IDX_OK(v, e, (uint32_t)v.N + 1u)) return;
   for (uint32_t k = s; k < e; k++) {
     const uint32_t j = v.tmp[k];
     rank += (j > (uint32_t)i) ? 1u : 0u;
     solids += (j < (uint32_t)v.S) ? 1u : 0u;
   }
+  if (!UPBD_IDX_OK(v, s + rank, v.N)) return;
   v.entries[s + rank] = (uint32_t)i;
   if (v.spos) {  // the stateless grid build has no bucket-ordered copies
     v.slot[i] = s + rank;
@@ -367,6 +370,7 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
             // own slot, which pair() skips (d2 = 0)
             const uint32_t r = (c + w < cnt[u]) ? __ldg(&nbr[((uint32_t)(l0 + u) * NL + c + w) * NS]) : e0;
             e[w] = (r & NBR_IN) ? (r & ~NBR_IN) : e0;
+            if (!UPBD_IDX_OK(v, e[w], NS)) e[w] = e0;  // out of range: the own slot (skipped, reported)
           }
 #pragma unroll
           for (int w = 0; w < 4; w++) {
@@ -445,7 +449,10 @@ __device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParam
   uint32_t* __restrict__ mark = v.mark;
   lane_strided<0, G>(v, ch, lane, act, [&](uint32_t e) { return sfp[e]; }, [&](uint32_t e, const real4& pj) {
     const real ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-    if (ex * ex + ey * ey + ez * ez < lim2) mark[v.entries[e]] = 1u;
+    if (ex * ex + ey * ey + ez * ez < lim2) {
+      const uint32_t j = v.entries[e];
+      if (UPBD_IDX_OK(v, j, v.N)) mark[j] = 1u;
+    }
   });
 }
 
@@ -503,6 +510,7 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
     for (uint32_t k = st + lane; k < en; k += GL) {
       const uint32_t ci = __ldg(&ids[k]);
       const uint32_t other = __ldg(&v.adj_other[k]);
+      if (!UPBD_IDX_OK(v, ci, v.C) || !UPBD_IDX_OK(v, other, v.S)) continue;
       const real s = __ldg(&v.adj_scale[k]);
       const real4 po = pos[other];
       const uint2 rw = *reinterpret_cast<const uint2*>(&cons[ci].z);  // rest bits, alive
@@ -607,6 +615,7 @@ __device__ __forceinline__ bool lattice_adjacent(const SimView& v, uint32_t i, u
 __device__ __forceinline__ bool is_bonded(const SimView& v, uint32_t i, uint32_t j) {
   const uint32_t* ids = v.adj + v.S + 1;
   for (uint32_t k = v.adj[i]; k < v.adj[i + 1]; k++) {
+    if (!UPBD_IDX_OK(v, ids[k], v.C)) continue;
     const uint4 c = v.cons[ids[k]];
     if (c.w != 0u && (c.x == j || c.y == j)) return true;
   }
@@ -663,6 +672,7 @@ __device__ __forceinline__ void b_solid_contacts(const SimView& v, const DevPara
   const uint32_t n = v.ccount[i];
   for (uint32_t k = 0; k < n; k++) {
     const uint32_t j = v.clist[(size_t)i * C_K + k];
+    if (!UPBD_IDX_OK(v, j, v.S)) continue;
     const real4 pj = v.pos[j];
     const real ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
     const real rsum = solid_rsum(v, P, i, j);
@@ -712,8 +722,12 @@ __device__ __forceinline__ void b_solve_tets(const SimView& v, const DevParams* 
   real cx = 0.f, cy = 0.f, cz = 0.f;
   for (uint32_t k = v.tet_adj[i]; k < v.tet_adj[i + 1]; k++) {
     const uint32_t t = ids[k];
+    if (!UPBD_IDX_OK(v, t, v.NT)) continue;
     const uint32_t ia = v.tet_idx[4 * t], ib = v.tet_idx[4 * t + 1], ic = v.tet_idx[4 * t + 2],
                    id = v.tet_idx[4 * t + 3];
+    if (!UPBD_IDX_OK(v, ia, v.S) || !UPBD_IDX_OK(v, ib, v.S) || !UPBD_IDX_OK(v, ic, v.S) ||
+        !UPBD_IDX_OK(v, id, v.S))
+      continue;
     const real V0 = v.tet_vol[t];
     if (V0 <= 0.f) continue;
     const real4 pa = v.pos[ia], pb = v.pos[ib], pc = v.pos[ic], pd = v.pos[id];
@@ -769,6 +783,7 @@ __device__ __forceinline__ void b_solve_tets(const SimView& v, const DevParams* 
 __device__ __forceinline__ void bond_update(const SimView& v, const DevParams* __restrict__ P, int ci) {
   const uint4 c = v.cons[ci];
   if (c.w == 0u) return;
+  if (!UPBD_IDX_OK(v, c.x, v.S) || !UPBD_IDX_OK(v, c.y, v.S)) return;
   const real4 pa = v.pos[c.x], pb = v.pos[c.y];
   const real ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
   const real d = r_sqrt(dot3(ex, ey, ez, ex, ey, ez));
@@ -796,6 +811,7 @@ __device__ __forceinline__ void tet_update(const SimView& v, const DevParams* __
   for (int p = 0; p < 3; p++)
     for (int q = p + 1; q < 4; q++) {
       const uint32_t a = v.tet_idx[4 * t + p], b = v.tet_idx[4 * t + q];
+      if (!UPBD_IDX_OK(v, a, v.S) || !UPBD_IDX_OK(v, b, v.S)) return;
       const real4 pa = v.pos[a], pb = v.pos[b];
       const real ex = pa.x - pb.x, ey = pa.y - pb.y, ez = pa.z - pb.z;
       const real d = r_sqrt(dot3(ex, ey, ez, ex, ey, ez));
@@ -1134,7 +1150,10 @@ __device__ __forceinline__ void b_xsph(const SimView& v, const DevParams* __rest
       uint32_t e[XCH];
       PV pv[XCH];
 #pragma unroll
-      for (int w = 0; w < XCH; w++) e[w] = (c + w < cnt) ? (__ldg(&nbr[(c + w) * NS]) & ~NBR_IN) : myslot;
+      for (int w = 0; w < XCH; w++) {
+        e[w] = (c + w < cnt) ? (__ldg(&nbr[(c + w) * NS]) & ~NBR_IN) : myslot;
+        if (!UPBD_IDX_OK(v, e[w], NS)) e[w] = myslot;  // out of range: the own slot (skipped, reported)
+      }
 #pragma unroll
       for (int w = 0; w < XCH; w++) pv[w] = load(e[w]);
 #pragma unroll

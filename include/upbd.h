@@ -72,6 +72,7 @@ extern "C" {
 #define UPBD_HEALTH_NAN      1u
 #define UPBD_HEALTH_TIMEOUT  2u
 #define UPBD_HEALTH_OVERFLOW 4u
+#define UPBD_HEALTH_BOUNDS   8u  /* checked build only: an index out of range was skipped */
 
 /* Scene layout: GpuSim DEFAULTS (src/gpu/sim.js:20-33) and
  * _buildHostData (src/gpu/sim.js:98-214). */
