@@ -1320,18 +1320,18 @@ int upbd_profile_graph_floor(upbd_sim* s, double dt, int32_t substeps, int32_t r
   ce = cudaGraphInstantiate(&ge, g, 0);
   cudaGraphDestroy(g);
   if (ce != cudaSuccess) return fail(s, UPBD_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
-  for (int k = 0; k < 3; k++) cudaGraphLaunch(ge, s->stream);
-  cudaEventRecord(a, s->stream);
-  for (int k = 0; k < reps; k++) cudaGraphLaunch(ge, s->stream);
-  cudaEventRecord(b, s->stream);
-  ce = cudaEventSynchronize(b);
+  cudaEvent_t a = nullptr, b = nullptr;
+  ce = cudaEventCreate(&a);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&b);
+  for (int k = 0; k < 3 && ce == cudaSuccess; k++) ce = cudaGraphLaunch(ge, s->stream);
+  if (ce == cudaSuccess) ce = cudaEventRecord(a, s->stream);
+  for (int k = 0; k < reps && ce == cudaSuccess; k++) ce = cudaGraphLaunch(ge, s->stream);
+  if (ce == cudaSuccess) ce = cudaEventRecord(b, s->stream);
+  if (ce == cudaSuccess) ce = cudaEventSynchronize(b);
   float t = 0.f;
   if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, a, b);
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
   cudaGraphExecDestroy(ge);
   if (ce != cudaSuccess) return fail(s, UPBD_ERR_CUDA, std::string("floor timing: ") + cudaGetErrorString(ce));
   *floor_ms = (double)t / reps;

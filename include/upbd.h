@@ -152,7 +152,8 @@ typedef struct upbd_info {
 
 /* Device pointers of the resident state, for a zero-copy consumer on the
  * same device (replaces the renderer's direct use of sim.buf.pos/flags,
- * src/gpu/render.js:142-151). Valid until upbd_destroy. */
+ * src/gpu/render.js:142-151). Valid until upbd_destroy. (In the test-only
+ * FP64 build, libupbd_fp64.so, the float4/float2 rows are double4/double2.) */
 typedef struct upbd_device_ptrs {
   void* pos;      /* float4[total] */
   void* prev;     /* float4[total] */
