@@ -167,14 +167,33 @@ def reduce_over_ranks(pg, ms: float, units: float, device) -> tuple[float, float
     return float(t.item()), float(u.item())
 
 
+def o1_settled(o1, sc) -> str:
+    """Loads the CPU solver's own state at frame 300 of the default scene
+    (oracle/data, made by oracle/make_settled_o1.py) into an O1 replica of
+    it: the settled pool the GPU line is timed on. Returns the start it gave
+    the replica, for the JSON line."""
+    settled = ROOT / "oracle" / "data" / "gpu_default_o1_frame300.npz"
+    if not settled.exists():
+        return "its initial state"
+    z = np.load(settled)
+    o1.set("pos", z["pos"])
+    o1.set("prev", z["pos"])  # rewritten from pos at the start of every substep
+    o1.set("vel", z["vel"])
+    o1.set("active", z["active"])
+    o1.set("consRest", z["consRest"])
+    o1.set("consAlive", z["consAlive"])
+    return f"the CPU solver's own state at frame {int(z['frames'])} (slice at frame {sc.slice_frame})"
+
+
 def cpu_baseline(seconds: float = 12.0) -> dict:
     """O1 (the CPU solver restated with its JavaScript numerics) on the
-    default scene, one thread, a bounded number of substeps from the
-    scene's initial state."""
+    default scene, one thread, a bounded number of substeps from the CPU
+    solver's own settled state (o1_settled)."""
     from fluidphysics_b200 import scenes as S
     from oracle.oracle import o1_from_scene
     sc = S.gpu_default(frames=1)
     o1 = o1_from_scene(sc)
+    start = o1_settled(o1, sc)
     h = sc.dt / sc.substeps
     n_sub = 0
     parts = 0
@@ -188,8 +207,8 @@ def cpu_baseline(seconds: float = 12.0) -> dict:
         if el >= seconds or n_sub >= 500:
             break
     return {"value": parts / el, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{n_sub} substeps of gpu_default (8,000 body + 65,536 fluid) from its initial "
-                      f"state, O1 restatement of src/solver.js, 1 thread, {el:.1f} s"}
+            "sample": f"{n_sub} substeps of gpu_default (8,000 body + 65,536 fluid) from {start}, "
+                      f"O1 restatement of src/solver.js, 1 thread, {el:.1f} s"}
 
 
 def run_reference(args) -> None:
@@ -197,7 +216,10 @@ def run_reference(args) -> None:
     src/solver.js: no JavaScript engine exists on this host) on all the host's
     cores: the CPU solver is sequential (Gauss-Seidel), so every core steps
     its own replica of the default scene and the line reports the replicas'
-    total particle-substeps over the wall time. A step is one substep."""
+    total particle-substeps over the wall time. A step is one substep. The
+    replicas start from the CPU solver's own state at frame 300 of the
+    default scene (oracle/data, made by oracle/make_settled_o1.py), the
+    settled pool the GPU arm is timed on."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
@@ -209,6 +231,7 @@ def run_reference(args) -> None:
     h = sc.dt / sc.substeps
     cores = max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
     reps = [o1_from_scene(sc) for _ in range(cores)]
+    start = [o1_settled(o, sc) for o in reps][0]
     parts = [0] * cores
 
     def work(k: int, steps: int, count: bool) -> None:
@@ -230,15 +253,15 @@ def run_reference(args) -> None:
     run_all(args.warmup, False)
     el = run_all(args.steps, True)
     v = sum(parts) / el
-    sample = (f"{args.steps} substeps of gpu_default on each of {cores} replicas, one per host thread, with "
-              "O1, the restatement of src/solver.js (no JavaScript engine on this host)")
+    sample = (f"{args.steps} substeps of gpu_default from {start} on each of {cores} replicas, one per host "
+              "thread, with O1, the restatement of src/solver.js (no JavaScript engine on this host)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded jittered fluid block, lattice body)",
         "config": {"workload": "gpu_default: 20^3 body (93,556 constraints) + 65,536 fluid, 1 substep "
-                               "per step (h = 1/300), CPU solver", "substeps_per_step": 1,
+                               f"per step (h = 1/300), CPU solver, from {start}", "substeps_per_step": 1,
                    "replicas": cores},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
