@@ -335,8 +335,65 @@ class GpuSim:
         c = self.sim.read_constraints()
         return {"alive": int(c[:, 3].sum()), "total": self.NUM_CONS}
 
+    def metrics(self) -> dict:
+        """The app's health probe, window.__sim.metrics() (src/gpu/main.js:542-567)."""
+        return state_metrics(self.readState(), self.SOLID_N)
+
+    def cutLine(self, x: float, eye) -> None:
+        """window.__sim.cutLine(x) (src/gpu/main.js:568-578): a vertical slice
+        through the body at world x, queued as wedge segments from the eye
+        (the app's camera position) to targets (x, 0.6 + t, 0), t = -1.4 ..
+        1.4 by 0.1, one segment applied per frame."""
+        for o, d1, d2 in cut_line_segments(x, eye):
+            self.queueCut(o, d1, d2)
+
     def dispose(self) -> None:
         self.sim.close()
+
+
+def cut_line_segments(x: float, eye) -> list:
+    """The wedge segments of window.__sim.cutLine(x) (src/gpu/main.js:568-578)
+    from an eye position: (origin, previous direction, direction) for the
+    targets (x, 0.6 + t, 0), t = -1.4, -1.3, ... (the app's loop bound
+    t <= 1.4 on the double sum: 28 targets, 27 segments)."""
+    o = np.asarray(eye, dtype=np.float64)
+    out, prev = [], None
+    t = -1.4
+    while t <= 1.4:
+        d = np.array([x, 0.6 + t, 0.0]) - o
+        d /= np.linalg.norm(d)
+        if prev is not None:
+            out.append((o, prev, d))
+        prev = d
+        t += 0.1
+    return out
+
+
+def state_metrics(st: dict, solid_n: int) -> dict:
+    """Aggregates of window.__sim.metrics() (src/gpu/main.js:542-567) over a
+    state read back as upbd_read_state returns it: the body's lowest and
+    highest y, non-finite count and mean speed; the active fluid's count,
+    non-finite count, highest y, percentage below y = 0.5 (pooled) and mean
+    speed."""
+    pos = st["pos"].astype(np.float64)
+    vel = st["vel"].astype(np.float64)
+    sy = pos[:solid_n, 1]
+    sok = np.isfinite(sy)
+    ssp = np.sqrt((vel[:solid_n, :3] ** 2).sum(axis=1))
+    act = (st["flags"][solid_n:] & 1) == 1
+    fy = pos[solid_n:, 1][act]
+    fok = np.isfinite(fy)
+    fsp = np.sqrt((vel[solid_n:, :3][act][fok] ** 2).sum(axis=1))
+    fn = int(fok.sum())
+    return {
+        "solid": {"minY": float(sy[sok].min()) if sok.any() else 1e9,
+                  "maxY": float(sy[sok].max()) if sok.any() else -1e9,
+                  "bad": int((~sok).sum()), "avgSpeed": float(ssp[sok].sum() / max(solid_n, 1))},
+        "fluid": {"n": fn, "bad": int((~fok).sum()), "maxY": float(fy[fok].max()) if fn else -1e9,
+                  "pooledPct": int(np.floor(100 * (fy[fok] < 0.5).sum() / fn + 0.5)) if fn else 0,
+                  "avgSpeed": float(fsp.mean()) if fn else 0.0},
+        "gpu": None,
+    }
 
 
 class Solver:
