@@ -292,7 +292,7 @@ def run_batched(args, stream, hbm: float) -> dict:
             cb.step(dt, nsub)
         cb.sync()
         best_r, table_r = B.autotune(cb, dict(zip(cids, cand_scs)), dt, nsub, frames=3,
-                                     block_threads=(128, 256), ctas_per_sm=(8, 16), cell_scales=(1.0, 1.1),
+                                     block_threads=(128, 256), ctas_per_sm=(32, 64, 128, 256), cell_scales=(1.0, 1.1),
                                      warm_frames=1)
         tried.append((best_r.ms_per_frame, rule, best_r, table_r, cb, cids, cand_scs))
     tried.sort(key=lambda x: x[0])

@@ -638,7 +638,7 @@ int upbd_batch_create(const upbd_batch_desc* d, upbd_batch** out) {
   if (d->max_scenes < 1 || d->max_scenes > 65536) return bfail(nullptr, UPBD_ERR_INVALID, "max_scenes out of range");
   if (d->block_threads != 64 && d->block_threads != 128 && d->block_threads != 256)
     return bfail(nullptr, UPBD_ERR_INVALID, "block_threads must be 64, 128 or 256");
-  if (d->ctas_per_sm < 1 || d->ctas_per_sm > 64) return bfail(nullptr, UPBD_ERR_INVALID, "ctas_per_sm out of range");
+  if (d->ctas_per_sm < 1 || d->ctas_per_sm > 256) return bfail(nullptr, UPBD_ERR_INVALID, "ctas_per_sm out of range");
   if (d->solid_iters < 0 || d->solid_iters > 1000) return bfail(nullptr, UPBD_ERR_INVALID, "solid_iters out of range");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -794,7 +794,7 @@ int upbd_batch_set_tuning(upbd_batch* b, int32_t block_threads, int32_t ctas_per
   if (!b) return UPBD_ERR_INVALID;
   if (block_threads != 64 && block_threads != 128 && block_threads != 256)
     return bfail(b, UPBD_ERR_INVALID, "block_threads must be 64, 128 or 256");
-  if (ctas_per_sm < 1 || ctas_per_sm > 64) return bfail(b, UPBD_ERR_INVALID, "ctas_per_sm out of range");
+  if (ctas_per_sm < 1 || ctas_per_sm > 256) return bfail(b, UPBD_ERR_INVALID, "ctas_per_sm out of range");
   if (block_threads != b->bt) b->dirty = true;  // tile counts change with the block size
   b->bt = block_threads;
   b->cps = ctas_per_sm;

@@ -34,7 +34,7 @@ typedef struct upbd_batch_desc {
   uint32_t features;      /* UPBD_FEAT_* of every scene (scene desc must agree) */
   int32_t max_scenes;     /* capacity of the scene table, 1..65536 */
   int32_t block_threads;  /* threads per CTA of the per-particle passes: 64, 128 or 256 */
-  int32_t ctas_per_sm;    /* persistent grid of every pass: CTAs per SM, 1..64 */
+  int32_t ctas_per_sm;    /* persistent grid of every pass: CTAs per SM, 1..256 */
   uint64_t hbm_budget;    /* device bytes of scene state the batch may hold; 0 = no limit */
   int32_t reserved[8];
 } upbd_batch_desc;
