@@ -230,7 +230,7 @@ int launch_substep(upbd_sim* s, int last) {
   UPBD_KCK(s);
   if (last < UPBD_PASS_APPLY_FLUID) return UPBD_OK;
   if (!fold && (last < UPBD_PASS_SOLID || iters == 0)) {
-    PROF(s, K_APPLY_FLUID, k_apply_fluid<<<blocks_for(v.F), 256, 0, st>>>(v));
+    PROF(s, K_APPLY_FLUID, k_apply_fluid<<<blocks_for(v.F), 256, 0, st>>>(v, P));
     L++;
     if (last < UPBD_PASS_SOLID) return UPBD_OK;
   }

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256) kb_disp(BatchArgs a) {
   batch_loop<D_DISP, false>(a, UPBD_BODY { b_disp<APPLY>(v, P, vb); });
 }
 __global__ void __launch_bounds__(256) kb_apply_fluid(BatchArgs a) {
-  batch_loop<D_F, false>(a, UPBD_BODY { b_apply_fluid(v, vb); });
+  batch_loop<D_F, false>(a, UPBD_BODY { b_apply_fluid(v, P, vb); });
 }
 template <bool APPLY_FLUID, int OUT>
 __global__ void __launch_bounds__(256, 6) kb_solid_solve(BatchArgs a, int it) {

@@ -68,7 +68,9 @@ template <bool APPLY>
 __global__ void __launch_bounds__(256) k_disp(SimView v, const DevParams* __restrict__ P) {
   b_disp<APPLY>(v, P, blockIdx.x);
 }
-__global__ void __launch_bounds__(256) k_apply_fluid(SimView v) { b_apply_fluid(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_apply_fluid(SimView v, const DevParams* __restrict__ P) {
+  b_apply_fluid(v, P, blockIdx.x);
+}
 template <bool APPLY_FLUID, int OUT>
 __global__ void __launch_bounds__(256) k_solid_solve(SimView v, const DevParams* __restrict__ P, int solid_pad, int it) {
   b_solid_solve<APPLY_FLUID, OUT>(v, P, solid_pad, it, blockIdx.x);

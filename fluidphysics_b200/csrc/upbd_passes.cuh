@@ -286,6 +286,25 @@ __device__ __forceinline__ void b_density(const SimView& v, const DevParams* __r
   }
 }
 
+// Contact marks (mark_fluid_near below) find a fluid particle from the
+// solid's side, through the bucket the grid build put it in; the particle's
+// own contact walk runs around the cell it is in after its displacement. A
+// displacement that carries it into another cell can bring it within contact
+// range of a solid two cells from its grid cell, which no mark walk reaches,
+// so the pass that applies the fluid's move (from o, the position the grid
+// was built from, to p) marks such a particle itself and it walks. Every
+// particle that kept its cell and is in range of a solid is in a bucket of
+// the 27 around that solid's cell, where the mark walk finds it.
+__device__ __forceinline__ void mark_if_cell_changed(const SimView& v, const DevParams* __restrict__ P, int i,
+                                                     const real4& o, const real4& p) {
+  if (!P->use_mark) return;
+  const double inv = P->inv_cell;
+  const bool same = floor(__dmul_rn((double)o.x, inv)) == floor(__dmul_rn((double)p.x, inv)) &&
+                    floor(__dmul_rn((double)o.y, inv)) == floor(__dmul_rn((double)p.y, inv)) &&
+                    floor(__dmul_rn((double)o.z, inv)) == floor(__dmul_rn((double)p.z, inv));
+  if (!same) v.mark[i] = 1u;  // also for a coordinate that is not finite
+}
+
 // fluidDisp, src/gpu/wgsl.js:281-316, DL threads per slot over the density
 // pass's lists (same positions). Thread h of a slot takes lanes h*GLF/DL ..
 // (h+1)*GLF/DL - 1: lane l's in-range neighbours (its NBR_IN entries) in its
@@ -415,21 +434,24 @@ __device__ __forceinline__ void b_disp(const SimView& v, const DevParams* __rest
     const real4 p = make_real4(pi.x + sx, pi.y + sy, pi.z + sz, pi.w);
     v.pos[i] = p;
     v.sfp[e0] = p;
+    mark_if_cell_changed(v, P, (int)i, pi, p);
   } else {
     v.delta[i] = make_real4(sx, sy, sz, 1.0f);
   }
 }
 
 // applyDeltaFluid, src/gpu/wgsl.js:318-323 (standalone form)
-__device__ __forceinline__ void b_apply_fluid(const SimView& v, uint32_t vb) {
+__device__ __forceinline__ void b_apply_fluid(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   const int i = v.S + (int)UPBD_VTID;
   if (i >= v.N) return;
   if (!(v.flags[i] & F_ACTIVE)) return;
-  real4 p = v.pos[i];
+  const real4 o = v.pos[i];
+  real4 p = o;
   const real4 d = v.delta[i];
   p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
   v.pos[i] = p;
   v.sfp[v.slot[i]] = p;
+  mark_if_cell_changed(v, P, i, o, p);
 }
 
 // ------------------------------------------------------------------ solids
@@ -485,11 +507,13 @@ __device__ __forceinline__ void b_solid_solve(const SimView& v, const DevParams*
   if (t >= solid_pad) {
     const int i = v.S + (t - solid_pad);
     if (APPLY_FLUID && i < v.N && (v.flags[i] & F_ACTIVE)) {
-      real4 p = v.pos[i];
+      const real4 o = v.pos[i];
+      real4 p = o;
       const real4 d = v.delta[i];
       p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
       v.pos[i] = p;
       v.sfp[v.slot[i]] = p;
+      mark_if_cell_changed(v, P, i, o, p);
     }
     return;
   }

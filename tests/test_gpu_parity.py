@@ -281,6 +281,71 @@ def test_substeps_within_tolerance_product_build(which, request):
     print(which, errs)
 
 
+def crossing_state(sc, cluster=12):
+    """The CPU scene with its lattice moved so that a surface solid j sits
+    1 mm below a cell boundary in x, every fluid particle inactive but one,
+    i, 2 mm into the cell two cells beyond j's, and a packed cluster right
+    behind i whose pressure pushes i back towards the lattice by the
+    displacement limit (0.35 H) within one substep: i crosses into the cell
+    next to j's and ends within contact range of j. Rows are float32-exact."""
+    o2 = o2_from_scene(sc)
+    st = o2.read_state()
+    pos, flags = st["pos"].copy(), st["flags"].copy()
+    n_s, c = sc.solid_n, sc.params.cell_size
+    sol = pos[:n_s, :3]
+    ctr = sol.mean(axis=0)
+    j = int(np.argmax(sol[:, 0] - 1e-3 * (np.abs(sol[:, 1] - ctr[1]) + np.abs(sol[:, 2] - ctr[2]))))
+    Y = np.floor(sol[j, 0] / c) + 3
+    pos[:n_s, 0] += (Y + 1) * c - 0.001 - sol[j, 0]
+    flags[n_s:] = 0
+    i = n_s
+    pos[i, :3] = [(Y + 2) * c + 0.002, pos[j, 1], pos[j, 2]]
+    flags[i] = 1
+    for m in range(cluster):
+        a = 2 * np.pi * m / cluster
+        pos[i + 1 + m, :3] = [pos[i, 0] + 0.04, pos[j, 1] + 0.01 * np.cos(a), pos[j, 2] + 0.01 * np.sin(a)]
+        flags[i + 1 + m] = 1
+    f32 = lambda a: a.astype(np.float32).astype(np.float64)
+    return dict(pos=f32(pos), prev=f32(st["prev"]), vel=np.zeros_like(st["vel"]), density=f32(st["density"]),
+                flags=flags), i, j, Y
+
+
+@pytest.mark.parametrize("variant", ["parity", "product"])
+def test_contact_after_cell_change(variant):
+    """Contact marks reach fluid from the solids' side, through the bucket
+    the grid build put each fluid particle in, while a fluid particle's own
+    contact walk runs around the cell its displacement moved it to. Here the
+    displacement carries fluid particle i into the next cell and within
+    contact range of solid j, two cells from i's grid cell, which no mark
+    walk reaches: the reference's contact pass (the oracle) gives i that
+    contact, and so must the library (the pass that applies the displacement
+    marks a particle that changed cell). The substep matches the oracle: bit
+    for bit in the parity build, within tolerance in the product build."""
+    sc = S.cpu_scene()
+    st, i, j, Y = crossing_state(sc)
+    c, h = sc.params.cell_size, sc.dt / sc.substeps
+    o2 = o2_from_scene(sc)
+    # the scenario holds in the oracle: i changes cell and meets j
+    o2.write_state(**st)
+    o2.substep_partial(h, L.PASS["APPLY_FLUID"])
+    p1 = o2.read_state()["pos"][i, :3]
+    assert np.floor(st["pos"][i, 0] / c) - Y == 2 and np.floor(p1[0] / c) - Y == 1
+    o2.write_state(**st)
+    o2.substep_partial(h, L.PASS["CONTACTS"])
+    assert o2.read_delta()[i, 3] >= 1.0, "no contact for i in the oracle"
+    o2.write_state(**st)
+    o2.substep_partial(h, 1000)
+    sim = sim_from_scene(sc, variant)
+    load_state(sim, st)
+    sim.substep_partial(h, 1000)
+    g, r = sim.read_state(), o2.read_state()
+    if variant == "parity":
+        assert_states_equal(g, r, "substep with a cell change into contact")
+    else:
+        assert_states_close(g, r, "substep with a cell change into contact")
+    sim.close()
+
+
 @pytest.mark.parametrize("which", ["c1_settled", "c2_settled"])
 def test_fp64_build_substeps_match_fp64_oracle(which, request):
     """The test-only FP64 build (the same pass bodies on double) against the
