@@ -14,7 +14,10 @@ centre at frame 60 of the timed run.
                drives it: per frame the uniform block goes host->device and
                positions + flags come back device->host into pinned memory
   roofline     the dominant kernel's algorithmic bytes per launch over its
-               average event-timed duration, against the measured HBM peak
+               average event-timed duration, against the measured HBM peak;
+               `issue` beside it: that kernel's warp instructions per launch
+               (committed ncu count) over the same duration, against one
+               warp instruction per scheduler per cycle at the sampled clock
   cpu_baseline the CPU solver restated (oracle O1, src/solver.js numerics),
                single thread as JavaScript runs, on a bounded sample
   clocks       nvidia-smi samples taken during the timed region
@@ -85,6 +88,22 @@ def ncu_traffic(kernel: str, workload: str):
     """DRAM bytes per launch from a committed ncu summary, if one exists:
     profiles/traffic.txt lines `kernel workload bytes_per_launch`."""
     f = ROOT / "profiles" / "traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+def ncu_instructions(kernel: str, workload: str):
+    """Warp instructions per launch from a committed ncu summary, if one
+    exists: profiles/instructions.txt lines `kernel workload count`."""
+    f = ROOT / "profiles" / "instructions.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -757,6 +776,18 @@ def main() -> None:
                 "traffic": ncu_traffic(dom, "gpu_default"),
                 "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}
                             for k, v in sorted(per_kernel.items(), key=lambda x: -x[1]["share"])}}
+    # the bound the gathers actually meet on L2-resident data: instruction
+    # issue (one warp instruction per scheduler per cycle, 4 schedulers per SM)
+    wi = ncu_instructions(dom, "gpu_default")
+    if wi:
+        sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+        roofline["issue"] = {"warp_inst_per_launch": wi, "avg_launch_us": dk["avg_us"],
+                             "achieved": wi / (dk["avg_us"] * 1e-6) / 1e9, "unit": "G warp-instructions/s",
+                             "sms": sm_count, "source": "profiles/instructions.txt (ncu smsp__inst_executed.sum)"}
+        mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+        if mhz:  # the SM clock sampled under load in the timed region
+            peak_i = sm_count * 4 * float(mhz) * 1e6 / 1e9
+            roofline["issue"].update(peak=peak_i, frac=roofline["issue"]["achieved"] / peak_i, sm_mhz=mhz)
     # whole-step roofline: the substep's algorithmic bytes at the measured rate
     B_sub = (240 * n_act + 200 * n_fl + 8 * T + sc.desc.solid_iters * (84 * info.solid_n + 24 * info.num_cons)
              + 20 * info.num_cons)
