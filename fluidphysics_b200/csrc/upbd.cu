@@ -190,9 +190,11 @@ int launch_substep(upbd_sim* s, int last) {
   // pass of the grid build or the fluid gathers writes, so they run on the
   // side stream meanwhile; the last one also writes the solids' slot copies,
   // so it waits for the grid build, and still runs beside density and
-  // displacement (they read fluid slots only); the contact marks, which read
-  // the displaced fluid, follow on the main stream. Eager per-kernel timing
-  // keeps one stream.
+  // displacement (they read fluid slots only), followed there by the contact
+  // marks, which read the fluid's grid positions with a reach widened by the
+  // displacement limit (the pass that applies the displacement marks the
+  // particles that change cell). Eager per-kernel timing keeps one stream
+  // and marks from the displaced fluid after the solve.
   const bool fold = iters >= 2 && !tets && !scc && last >= UPBD_PASS_SOLID;
   const bool overlap = fold && !s->prof_on && s->side;
   const int solid_pad = ((v.S * GL + 31) / 32) * 32;  // lane threads of the solve, whole warps
@@ -215,6 +217,13 @@ int launch_substep(upbd_sim* s, int last) {
     UPBD_CK(s, cudaStreamWaitEvent(s->side, s->grid_ev, 0));
     k_solid_solve<false, SOLVE_FINAL><<<blocks_for(solid_pad), 256, 0, s->side>>>(v, P, solid_pad, iters - 1);
     L++;
+    // the contact marks from the solids' final positions and the fluid's
+    // grid positions (reach widened by the displacement limit), so they run
+    // here beside density and displacement rather than after them
+    if (v.S > 0) {
+      k_contact_mark<32, true><<<blocks_for((long long)v.S * 32), 256, 0, s->side>>>(v, P);
+      L++;
+    }
     UPBD_CK(s, cudaEventRecord(s->join_ev, s->side));
   }
   if (last < UPBD_PASS_DENSITY) return UPBD_OK;
@@ -243,9 +252,7 @@ int launch_substep(upbd_sim* s, int last) {
   const bool mark_in_apply = iters > 0 && !tets && !scc;
   if (fold) {
     if (overlap) {
-      UPBD_CK(s, cudaStreamWaitEvent(st, s->join_ev, 0));
-      PROF(s, K_APPLY_SOLID, k_contact_mark<32><<<blocks_for((long long)v.S * 32), 256, 0, st>>>(v, P));
-      L++;
+      UPBD_CK(s, cudaStreamWaitEvent(st, s->join_ev, 0));  // the solve and the marks
     } else {
       for (int it = 0; it < iters - 1; it++) {
         PROF(s, K_SOLID_SOLVE, k_solid_solve<false, SOLVE_STEP><<<blocks_for(solid_pad), 256, 0, st>>>(v, P, solid_pad, it));

@@ -79,9 +79,9 @@ template <bool MARK>
 __global__ void __launch_bounds__(256) k_apply_solid(SimView v, const DevParams* __restrict__ P) {
   b_apply_solid<MARK>(v, P, blockIdx.x);
 }
-template <int G>
+template <int G, bool FROM_GRID = false>
 __global__ void __launch_bounds__(256) k_contact_mark(SimView v, const DevParams* __restrict__ P) {
-  b_contact_mark<G>(v, P, blockIdx.x);
+  b_contact_mark<G, FROM_GRID>(v, P, blockIdx.x);
 }
 __global__ void __launch_bounds__(256) k_collect_contacts(SimView v, const DevParams* __restrict__ P) {
   b_collect_contacts(v, P, blockIdx.x);

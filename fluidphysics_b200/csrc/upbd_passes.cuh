@@ -460,14 +460,22 @@ __device__ __forceinline__ void b_apply_fluid(const SimView& v, const DevParams*
 // the contacts pass makes the exact test.
 // Every lane of the warp calls it (the hash is shared by shuffles); only
 // active solids walk.
-template <int G = GL>
+// FROM_GRID: the fluid's positions are those of the grid build (spos), from
+// before its displacement, which moves a particle by at most 0.35 H (the
+// displacement pass's clamp): the reach grows by that much (and a relative
+// 1e-3, far above the rounding of the positions), so every particle that
+// ends within contact range is marked, and the marks need not wait for the
+// displacement pass.
+template <int G = GL, bool FROM_GRID = false>
 __device__ __forceinline__ void mark_fluid_near(const SimView& v, const DevParams* __restrict__ P, real4 p,
                                                 bool act, int lane) {
   CellHash ch;
   group_cell_hash<G>(p.x, p.y, p.z, P->inv_cell, ch);
   const real rsum = P->solid_radius + P->fluid_radius;
-  const real lim2 = rsum * rsum * 1.00001f;
-  const real4* __restrict__ sfp = v.sfp;  // the fluid has moved by its displacement
+  const real reach = FROM_GRID ? (rsum + 0.35f * P->fluid_h) * 1.001f : rsum;
+  const real lim2 = reach * reach * 1.00001f;
+  // without FROM_GRID the fluid has moved by its displacement (sfp)
+  const real4* __restrict__ sfp = FROM_GRID ? v.spos : v.sfp;
   uint32_t* __restrict__ mark = v.mark;
   lane_strided<0, G>(v, ch, lane, act, [&](uint32_t e) { return sfp[e]; }, [&](uint32_t e, const real4& pj) {
     const real ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
@@ -606,13 +614,13 @@ __device__ __forceinline__ void b_apply_solid(const SimView& v, const DevParams*
 // Contact marking on its own (when the solve's last position update does not
 // carry it), G lanes per solid. Marks are a set, so the lane count is free:
 // a whole warp per solid makes the 27 bucket lookups one round.
-template <int G = GL>
+template <int G = GL, bool FROM_GRID = false>
 __device__ __forceinline__ void b_contact_mark(const SimView& v, const DevParams* __restrict__ P, uint32_t vb) {
   if (!P->use_mark) return;
   const int t = UPBD_VTID;
   const int i = t / G;
   const bool act = i < v.S && (v.flags[i] & F_ACTIVE);
-  mark_fluid_near<G>(v, P, act ? v.pos[i] : make_real4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (G - 1));
+  mark_fluid_near<G, FROM_GRID>(v, P, act ? v.pos[i] : make_real4(0.f, 0.f, 0.f, 0.f), act, threadIdx.x & (G - 1));
 }
 
 // latticeRest, src/gpu/wgsl.js:373-381
