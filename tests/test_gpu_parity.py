@@ -15,7 +15,7 @@ import pytest
 from fluidphysics_b200 import _lib as L
 from fluidphysics_b200 import scenes as S
 from fluidphysics_b200.sim import Sim, sim_from_scene
-from helpers import (assert_states_close, assert_states_equal, load_state, settled_state)
+from helpers import (assert_states_close, assert_states_equal, crossing_state, load_state, settled_state)
 from oracle.oracle import o1_from_scene, o2_from_scene
 
 pytestmark = pytest.mark.gpu
@@ -279,35 +279,6 @@ def test_substeps_within_tolerance_product_build(which, request):
         errs.append(assert_states_close(g, r, f"substep {k}"))
         load_state(sim, r, o2.read_constraints()[0])
     print(which, errs)
-
-
-def crossing_state(sc, cluster=12):
-    """The CPU scene with its lattice moved so that a surface solid j sits
-    1 mm below a cell boundary in x, every fluid particle inactive but one,
-    i, 2 mm into the cell two cells beyond j's, and a packed cluster right
-    behind i whose pressure pushes i back towards the lattice by the
-    displacement limit (0.35 H) within one substep: i crosses into the cell
-    next to j's and ends within contact range of j. Rows are float32-exact."""
-    o2 = o2_from_scene(sc)
-    st = o2.read_state()
-    pos, flags = st["pos"].copy(), st["flags"].copy()
-    n_s, c = sc.solid_n, sc.params.cell_size
-    sol = pos[:n_s, :3]
-    ctr = sol.mean(axis=0)
-    j = int(np.argmax(sol[:, 0] - 1e-3 * (np.abs(sol[:, 1] - ctr[1]) + np.abs(sol[:, 2] - ctr[2]))))
-    Y = np.floor(sol[j, 0] / c) + 3
-    pos[:n_s, 0] += (Y + 1) * c - 0.001 - sol[j, 0]
-    flags[n_s:] = 0
-    i = n_s
-    pos[i, :3] = [(Y + 2) * c + 0.002, pos[j, 1], pos[j, 2]]
-    flags[i] = 1
-    for m in range(cluster):
-        a = 2 * np.pi * m / cluster
-        pos[i + 1 + m, :3] = [pos[i, 0] + 0.04, pos[j, 1] + 0.01 * np.cos(a), pos[j, 2] + 0.01 * np.sin(a)]
-        flags[i + 1 + m] = 1
-    f32 = lambda a: a.astype(np.float32).astype(np.float64)
-    return dict(pos=f32(pos), prev=f32(st["prev"]), vel=np.zeros_like(st["vel"]), density=f32(st["density"]),
-                flags=flags), i, j, Y
 
 
 @pytest.mark.parametrize("variant", ["parity", "product"])

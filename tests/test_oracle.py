@@ -161,3 +161,87 @@ def test_emit_ring_buffer_wraps(oracle_lib):
     o2.step(1 / 60, 5)
     assert o2.fluid_next() == 256
     assert o2.active_count() <= 2600
+
+
+def _mark_rule_misses(sc, st, cons=None):
+    """Fluid particles that the oracle's contact pass (the reference's
+    contacts kernel restated) gives a contact but that the library's contact
+    marks would leave unmarked, so that they would skip their contact walk.
+    The library marks fluid particle i when (a) its displacement moved it into
+    another cell, or (b) some solid j, at its position after the solve, has
+    i's grid bucket among the 27 around its own cell and lies within
+    (r_s + r_f + 0.35 H) * 1.001 of i's grid position (float32 arithmetic,
+    as the kernels do). Returns (misses, contacted fluid, of which by (b) only
+    through the widened reach)."""
+    from fluidphysics_b200 import _lib as L
+    h = sc.dt / sc.substeps
+    p = sc.params
+    inv = 1.0 / p.cell_size
+    T = sc.desc.table_size
+    n_s = sc.solid_n
+    o2 = O2(sc.desc, sc.params)
+
+    def run(last):
+        o2.write_state(**st)
+        if cons is not None:
+            o2.write_constraints(cons)
+        o2.substep_partial(h, last)
+        return o2.read_state()
+
+    grid = run(L.PASS["GRID"])["pos"][:, :3].astype(np.float32)
+    moved = run(L.PASS["APPLY_FLUID"])["pos"][:, :3].astype(np.float32)
+    after = run(L.PASS["CONTACTS"])
+    delta = o2.read_delta()
+    fin = after["pos"][:n_s, :3].astype(np.float32)
+    act = (after["flags"] & 1).astype(bool)
+    cell = lambda q: np.floor(q.astype(np.float64) * inv)
+    rsum = np.float32(p.solid_radius) + np.float32(p.fluid_radius)
+    reach = (rsum + np.float32(0.35) * np.float32(p.fluid_h)) * np.float32(1.001)
+    lim2 = reach * reach * np.float32(1.00001)
+    fin_cells = cell(fin)
+    contacted = np.flatnonzero(act[n_s:] & (delta[n_s:, 3] > 0)) + n_s
+    misses, widened = [], 0
+    for i in contacted:
+        ci = cell(grid[i])
+        if (ci != cell(moved[i])).any():
+            continue  # (a)
+        bi = js_hash(ci[0], ci[1], ci[2], T)
+        near = np.flatnonzero(act[:n_s] & (np.abs(fin_cells - ci).max(axis=1) <= 2))
+        ok = False
+        for j in near:
+            d = fin[j] - grid[i]
+            if not (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < lim2):
+                continue
+            fc = fin_cells[j]
+            around = {js_hash(fc[0] + a, fc[1] + b, fc[2] + c, T) for a in (-1, 0, 1) for b in (-1, 0, 1)
+                      for c in (-1, 0, 1)}
+            if bi in around:
+                ok = True
+                dm = fin[j] - moved[i]
+                widened += int(not (float(np.dot(d, d)) < float(rsum) ** 2) and float(np.dot(dm, dm)) < float(rsum) ** 2)
+                break
+        if not ok:
+            misses.append(int(i))
+    return misses, len(contacted), widened
+
+
+@pytest.mark.parametrize("case", ["frame50", "frame60", "crossing"])
+def test_contact_mark_rules_cover_every_oracle_contact(oracle_lib, case):
+    """The marking rules of the library's contact pass, evaluated on the
+    oracle's own substep: every fluid particle the reference's contacts
+    kernel gives a contact is marked, in the CPU scene at frames 50 and 60
+    (the fluid block landing on the lattice: 170-180 fluid particles in
+    contact, some of them reached only through the widened reach) and in
+    the crossing case (a particle pushed across a cell boundary into
+    contact, which only the cell-change rule marks)."""
+    from helpers import crossing_state, settled_state
+    sc = S.cpu_scene()
+    if case.startswith("frame"):
+        _, st, cons = settled_state(sc, int(case[5:]))
+    else:
+        st, _, _, _ = crossing_state(sc)
+        cons = None
+    misses, n, widened = _mark_rule_misses(sc, st, cons)
+    print(case, "contacted fluid", n, "reached only through the widened reach", widened)
+    assert n > 0
+    assert not misses, misses[:8]
