@@ -29,6 +29,15 @@ def c1_settled():
 
 
 @pytest.fixture(scope="module")
+def c1_landing():
+    """The CPU scene at frame 50: the fluid block lands on the lattice (about
+    170 fluid particles in contact with solids, the contact marks at work)."""
+    sc = S.cpu_scene()
+    o2, st, cons = settled_state(sc, 50)
+    return sc, st, cons
+
+
+@pytest.fixture(scope="module")
 def c2_settled():
     sc = S.gpu_default(frames=1)
     o2, st, cons = settled_state(sc, 4)
@@ -241,7 +250,7 @@ PASSES = ["INTEGRATE", "GRID", "DENSITY", "DISP", "APPLY_FLUID", "SOLID", "BONDS
           "APPLY_ALL", "BOUNDS", "VELOCITY", "XSPH", "XSPH_APPLY"]
 
 
-@pytest.mark.parametrize("which", ["c1_settled", "c2_settled"])
+@pytest.mark.parametrize("which", ["c1_settled", "c1_landing", "c2_settled"])
 @pytest.mark.parametrize("pass_name", PASSES)
 def test_pass_bit_exact_parity_build(which, pass_name, request):
     sc, st, cons = request.getfixturevalue(which)
@@ -262,7 +271,7 @@ def test_pass_bit_exact_parity_build(which, pass_name, request):
         assert np.array_equal(o_g, o_o) and np.array_equal(e_g, e_o)
 
 
-@pytest.mark.parametrize("which", ["c1_settled", "c2_settled"])
+@pytest.mark.parametrize("which", ["c1_settled", "c1_landing", "c2_settled"])
 def test_substeps_within_tolerance_product_build(which, request):
     sc, st, cons = request.getfixturevalue(which)
     sim = sim_from_scene(sc, "product")
