@@ -199,6 +199,10 @@ def _mark_rule_misses(sc, st, cons=None):
     reach = (rsum + np.float32(0.35) * np.float32(p.fluid_h)) * np.float32(1.001)
     lim2 = reach * reach * np.float32(1.00001)
     fin_cells = cell(fin)
+    # the widened reach rests on the displacement pass's clamp (0.35 H)
+    fl = np.flatnonzero(act[n_s:]) + n_s
+    step = np.linalg.norm(moved[fl].astype(np.float64) - grid[fl].astype(np.float64), axis=1)
+    assert step.size == 0 or step.max() <= 0.35 * p.fluid_h * (1 + 1e-5), step.max()
     contacted = np.flatnonzero(act[n_s:] & (delta[n_s:, 3] > 0)) + n_s
     misses, widened = [], 0
     for i in contacted:
